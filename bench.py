@@ -1,0 +1,345 @@
+"""Benchmark: batched graph-state p(x) on B200 (single-instance throughput workload).
+
+Workload (one "step"): a seeded random 3-regular graph on n = 40 vertices with
+Haar-random SU(2) gates, scan order = the seeded random order with the largest
+max rank among 2048 seeds (r_max 20); p(x) for 65,536 uniform 40-bit strings in
+complex64 (float64 weights and sums), then the FP64 (complex128) recheck of every
+result.  Inputs are synthetic (seeded); there is no dataset.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1); every rank evaluates its own 65,536
+strings (weak scaling, no data-path collective); rank 0 prints one JSON line.
+``--impl reference`` times the reference's CPU executor (its NumPy sweep, restated
+in ``oracle/``) on all host cores, rank 0 only.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_QUBITS = 40
+GRAPH_SEED = 40
+BATCH = 65536
+ORDER_SEEDS = range(1000, 3048)
+TARGET_RANK = 22
+BITS_SEED = 1234
+
+
+def build_instance(pkg):
+    return pkg.instances.make_instance("reg3", N_QUBITS, GRAPH_SEED, pkg.rank_profile, target_rank=TARGET_RANK,
+                                       order_seeds=ORDER_SEEDS)
+
+
+def step_bytes(ranks, esize):
+    """Compulsory table traffic of one sweep: every input entry read once, every output
+    written once (step 0 reads the implicit unit table)."""
+    r_in = [0] + list(ranks[:-1])
+    return esize * sum((1 << a) * (j > 0) + (1 << b) for j, (a, b) in enumerate(zip(r_in, ranks)))
+
+
+def reference_bytes(ranks, esize):
+    """Byte model of the reference kernel: every input read twice (each output gathers
+    its pre-images), every output written once."""
+    r_in = [0] + list(ranks[:-1])
+    return esize * sum(2 * (1 << a) + (1 << b) for a, b in zip(r_in, ranks))
+
+
+# ----------------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------------- CPU legs
+def _cpu_worker(args):
+    g, u, order, bits_list = args
+    from oracle import scan_plan as sp
+    return [sp.amplitude(g, u, order, b) for b in bits_list]
+
+
+def cpu_oracle_rate(inst, bits, cores, per_core):
+    """Amplitudes/s of the reference's NumPy executor (restated in oracle/) on `cores`
+    spawned processes, each computing `per_core` amplitudes.  Returns (rate, amplitudes)."""
+    import multiprocessing as mp
+    sample = bits[:cores * per_core]
+    chunks = [(inst.g, inst.u, inst.order, [b.tolist() for b in sample[i::cores]]) for i in range(cores)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        pool.map(_cpu_worker, [(inst.g, inst.u, inst.order, [sample[0].tolist()])] * cores)  # import warm-up
+        t0 = time.perf_counter()
+        out = pool.map(_cpu_worker, chunks)
+        dt = time.perf_counter() - t0
+    amps = np.empty(len(sample), dtype=np.complex128)
+    for i in range(cores):
+        amps[i::cores] = out[i]
+    return len(sample) / dt, amps
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ----------------------------------------------------------------------------------- arms
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import __graft_entry__
+    pkg = __graft_entry__.package()
+    inst = build_instance(pkg)
+    cores = host_cores()
+    rng = np.random.default_rng(BITS_SEED)
+    bits = pkg.instances.uniform_bits(BATCH, N_QUBITS, rng)
+    per_core = 2
+    times = []
+    for it in range(args.warmup + args.steps):
+        rate, _ = cpu_oracle_rate(inst, bits[(it % 64) * cores * per_core:], cores, per_core)
+        if it >= args.warmup:
+            times.append(cores * per_core / rate)
+    value = cores * per_core * len(times) / sum(times)
+    line = {
+        "impl": "reference", "metric": "amplitudes_per_s (p(x), n=40 3-regular, complex64 + FP64 recheck)",
+        "value": value, "unit": "amplitudes/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded)",
+        "config": {"workload": "single-instance throughput: n=40 random 3-regular, Haar SU(2), "
+                               f"r_max {inst.rmax}, 65536 uniform strings (bounded sample per step)",
+                   "rmax": inst.rmax, "sum_states": inst.sum_states, "instance": inst.name},
+        "cpu_baseline": {"value": value, "unit": "amplitudes/s", "cores": cores, "kind": "port",
+                         "sample": f"{cores * per_core} amplitudes per step on {cores} processes "
+                                   "(oracle restatement of scan_plan.sweep_reference, complex128)"},
+        "e2e": {"value": value, "unit": "amplitudes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    import __graft_entry__
+    pkg = __graft_entry__.package()
+    inst = build_instance(pkg)
+    cores = host_cores()
+    device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=device)
+
+    plan = pkg.ScanPlan(N_QUBITS, pkg.edges_from_graph(inst.g), inst.order)
+    rng = np.random.default_rng(BITS_SEED + rank)
+    bits = pkg.instances.uniform_bits(BATCH, N_QUBITS, rng)
+    packed = pkg.pack_bits(bits, N_QUBITS)
+    eng64 = pkg.ScanEngine(plan, inst.u, device=device, precision="c64", batch_tile=512)
+    eng128 = pkg.ScanEngine(plan, inst.u, device=device, precision="c128", batch_tile=256)
+    d_bits = torch.from_numpy(packed.view(np.int64)).to(device)
+    v64, l64 = eng64.out_tensors(BATCH)
+    v128, l128 = eng128.out_tensors(BATCH)
+    stream = torch.cuda.current_stream(device)
+
+    def device_step():
+        eng64.run_bits(d_bits, v64, l64, stream=stream)
+        eng128.run_bits(d_bits, v128, l128, stream=stream)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(fn, k):
+        barrier()
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / 1e3)
+
+    for _ in range(args.warmup):
+        device_step()
+    torch.cuda.synchronize(device)
+    with ClockSampler(local_rank) as clocks:
+        t_step = timed(device_step, args.steps)
+    # Split of the step, and the FP64 recheck error.
+    t64 = timed(lambda: eng64.run_bits(d_bits, v64, l64, stream=stream), args.steps)
+    t128 = timed(lambda: eng128.run_bits(d_bits, v128, l128, stream=stream), args.steps)
+    p64 = np.abs(pkg.amplitudes_from(v64.cpu().numpy(), l64.cpu().numpy(), N_QUBITS)) ** 2
+    p128 = np.abs(pkg.amplitudes_from(v128.cpu().numpy(), l128.cpu().numpy(), N_QUBITS)) ** 2
+    if not (np.all(np.isfinite(p64)) and np.all(np.isfinite(p128))):
+        raise ArithmeticError("non-finite probability in the benchmark run")
+    recheck_err = float(np.max(np.abs(p64 - p128) / p128))
+
+    # End to end through the public API: pinned host bits in, host probabilities out.
+    h_bits = torch.from_numpy(packed.view(np.int64)).pin_memory()
+    h_v64 = torch.empty(BATCH, dtype=torch.complex64).pin_memory()
+    h_l64 = torch.empty(BATCH, dtype=torch.float64).pin_memory()
+    h_v128 = torch.empty(BATCH, dtype=torch.complex128).pin_memory()
+    h_l128 = torch.empty(BATCH, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        d_bits.copy_(h_bits, non_blocking=True)
+        device_step()
+        h_v64.copy_(v64, non_blocking=True)
+        h_l64.copy_(l64, non_blocking=True)
+        h_v128.copy_(v128, non_blocking=True)
+        h_l128.copy_(l128, non_blocking=True)
+
+    for _ in range(max(1, args.warmup // 2)):
+        e2e_step()
+    t_e2e = timed(e2e_step, args.steps)
+    h2d = packed.nbytes
+    d2h = BATCH * (8 + 8 + 16 + 8)
+
+    # Roofline of the scan-step kernels (dominant: they are all but three launches per tile).
+    b64 = step_bytes(inst.ranks, 8) * BATCH
+    b128 = step_bytes(inst.ranks, 16) * BATCH
+    peaks_path = ROOT / "MEASURED_PEAKS.json"
+    peak, peak_src = 6650.0, "fallback"
+    if peaks_path.exists():
+        peak, peak_src = float(json.loads(peaks_path.read_text())["hbm_gbs"]), "measured"
+    achieved = (b64 + b128) / (t_step / args.steps) / 1e9
+    traffic_path = ROOT / "profiles" / "scan_step_traffic.json"
+    traffic = json.loads(traffic_path.read_text()).get("dram_bytes_per_step") if traffic_path.exists() else None
+    groups64 = math.ceil(BATCH / 512)
+    groups128 = math.ceil(BATCH / 256)
+    launches = args.steps * ((groups64 + groups128) * (N_QUBITS + 2))
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            cpu_rate, cpu_amps = cpu_oracle_rate(inst, bits, cores, 2)
+            cpu = {"value": cpu_rate, "unit": "amplitudes/s", "cores": cores, "kind": "port",
+                   "sample": f"{2 * cores} amplitudes (complex128 NumPy sweep restated from the reference) "
+                             f"on {cores} spawned processes"}
+            p_cpu = np.abs(cpu_amps) ** 2
+            recheck_cpu = float(np.max(np.abs(p128[:len(p_cpu)] - p_cpu) / p_cpu))
+            cpu["parity_max_rel_err_vs_fp64"] = recheck_cpu
+        value = world * BATCH * args.steps / t_step
+        line = {
+            "metric": "amplitudes_per_s (p(x), n=40 3-regular, complex64 + FP64 recheck)",
+            "value": value, "unit": "amplitudes/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_step / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+            "data": "synthetic (seeded graph, gates and bitstrings)",
+            "config": {"workload": "single-instance throughput: n=40 random 3-regular, Haar SU(2), "
+                                   "65536 uniform 40-bit strings, complex64 + FP64 recheck of every result",
+                       "instance": inst.name, "rmax": inst.rmax, "sum_states": inst.sum_states,
+                       "batch_per_gpu": BATCH, "batch_tile": {"c64": 512, "c128": 256},
+                       "l2": "inputs larger than L2 (c64 tables 2 x 4 GiB, c128 2 x 4 GiB)",
+                       "parallelism": f"replicas x{world}"},
+            "split": {"c64_amplitudes_per_s": world * BATCH * args.steps / t64,
+                      "c128_amplitudes_per_s": world * BATCH * args.steps / t128,
+                      "fp64_recheck_max_prob_rel_err": recheck_err},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
+                         "algorithmic_bytes_per_step": b64 + b128,
+                         "reference_model_bytes_per_step": (reference_bytes(inst.ranks, 8)
+                                                            + reference_bytes(inst.ranks, 16)) * BATCH},
+            "e2e": {"value": world * BATCH * args.steps / t_e2e, "unit": "amplitudes/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+        }
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    global BATCH
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--batch", type=int, default=BATCH, help="bitstrings per GPU per step (profiling runs)")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", args.gpus if args.gpus == 1 else 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.warmup < 3:
+        raise SystemExit("warmup must be >= 3")
+    BATCH = args.batch
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

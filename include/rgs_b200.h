@@ -1,0 +1,112 @@
+/*
+ * rgs_b200 -- C ABI of the B200 graph-state probability and Born-sampling engine.
+ *
+ * Every entry point returns an int status (RGS_OK = 0), never throws, and
+ * records a message readable with rgs_last_error().  Device buffers are owned by
+ * the caller (plain device pointers); a plan owns only its small device tables.
+ * `stream` is a cudaStream_t passed as void*; NULL means the legacy default stream.
+ * No call synchronises the host unless its comment says so.
+ *
+ * Reference interfaces replaced (whyihaveyou/rgs70-classical-challenge,
+ * W/ = work/rgs_attack/) are cited beside each function.  The reference exposes
+ * only Python; these are the functions its Python layer would bind (see
+ * INTEGRATION.md for the ctypes stubs).
+ *
+ * Conventions.  Qubit/vertex q of a bitstring is bit q of a little-endian pair
+ * of uint64 words (bits[2*i] holds qubits 0..63, bits[2*i+1] qubits 64..127).
+ * Complex numbers are interleaved (re, im); complex128 = two doubles.
+ */
+#ifndef RGS_B200_H
+#define RGS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status codes */
+#define RGS_OK 0
+#define RGS_ERR_ARG 1          /* bad argument: Python ValueError                     */
+#define RGS_ERR_OOM 2          /* workspace or device memory too small: MemoryError    */
+#define RGS_ERR_CUDA 3         /* CUDA runtime error: RuntimeError                     */
+#define RGS_ERR_NONFINITE 4    /* NaN/Inf in a result: ArithmeticError                 */
+#define RGS_ERR_ZERO_NORM 5    /* zero or invalid normalisation: ArithmeticError       */
+#define RGS_ERR_TIMEOUT 6      /* a bounded device wait expired                        */
+#define RGS_ERR_UNSUPPORTED 7  /* plan/instance outside what the executor supports     */
+#define RGS_ERR_SINGULAR 8     /* GF(2) matrix not invertible (cut not full rank)      */
+
+/* Precision of the scan executor. */
+#define RGS_PREC_C64 0      /* complex64 tables, float64 weights and sums (W/upstream_scan/gpu_kernel.py:59-102) */
+#define RGS_PREC_C64_F32 1  /* complex64 tables, float32 weights and sums                                        */
+#define RGS_PREC_C128 2     /* complex128 tables and float64 math (W/upstream_scan/gpu_kernel_fp64.py:24-67)     */
+
+typedef struct rgs_plan rgs_plan;
+
+/* Library version string and the message of the last failing call in this thread. */
+const char* rgs_version(void);
+const char* rgs_last_error(void);
+/* Number of CUDA devices visible (0 without a GPU); never fails. */
+int rgs_device_count(void);
+
+/* ---------------------------------------------------------------- scan compiler
+ * Replaces make_plan / future_masks / byte_tables / kernel_combos
+ * (W/upstream_scan/scan_plan.py:45-55, 58-105, 133-145, 148-152) and the
+ * plan set-up of ScanOracle.__init__ (W/scan_oracle.py:12-18).
+ * edges: int32[n_edges][2]; order: int32[n] (a permutation); fixed: uint8[n] or
+ * NULL (vertices with deterministic y, the `fixed` argument of make_plan).
+ * Host-only: needs no GPU. */
+int rgs_plan_compile(int32_t n, int32_t n_edges, const int32_t* edges, const int32_t* order,
+                     const uint8_t* fixed, rgs_plan** out_plan);
+void rgs_plan_destroy(rgs_plan* plan);
+
+/* n, maximum rank, and whether the plan can be executed on a device (rank <= 61). */
+int rgs_plan_info(const rgs_plan* plan, int32_t* n, int32_t* rmax, int32_t* executable);
+/* Rank after each position: int32[n] (the profile returned by make_plan). */
+int rgs_plan_ranks(const rgs_plan* plan, int32_t* ranks);
+/* Future-neighbour masks: uint64[n][2] (lo, hi) (future_masks, scan_plan.py:45-55). */
+int rgs_plan_future_masks(const rgs_plan* plan, uint64_t* fut);
+/* Step j of the plan (Step, scan_plan.py:31-32).  Masks are 128-bit (lo, hi) pairs:
+ * beta uint64[2]; lcols uint64[r_out][2]; kernel uint64[2][2] (n_kernel <= 2 used). */
+int rgs_plan_step(const rgs_plan* plan, int32_t j, int32_t* v, int32_t* is_free, int32_t* r_in,
+                  int32_t* r_out, uint64_t* beta, uint64_t* lcols, int32_t* n_kernel, uint64_t* kernel);
+/* Byte tables of step j (byte_tables, scan_plan.py:133-145): uint64[nbytes][256][2]
+ * (lo, hi); pass tables = NULL to query nbytes. */
+int rgs_plan_step_tables(const rgs_plan* plan, int32_t j, uint64_t* tables, int32_t* nbytes);
+/* Rank profile without keeping a plan (cost model sum 2^r used by order search). */
+int rgs_rank_profile(int32_t n, int32_t n_edges, const int32_t* edges, const int32_t* order,
+                     const uint8_t* fixed, int32_t* ranks);
+
+/* ---------------------------------------------------------------- scan executor
+ * Replaces GPUMixin.alloc/_sweep (W/upstream_scan/gpu_kernel.py:111-170,
+ * gpu_kernel_fp64.py:76-135) and ScanOracle.amplitude (W/scan_oracle.py:25-29),
+ * batched over bitstrings.  For each bitstring i:
+ *     value[i] * exp(logscale[i]) * 2^(-n/2) = <x_i| (x)_q U_q |G>
+ * with the same power-of-two renormalisation as the reference, computed on the
+ * device (no per-step host round trip).
+ *
+ * Workspace: caller-owned device memory of at least
+ * rgs_scan_workspace_bytes(plan, batch_tile, precision) bytes; batch_tile is a
+ * power of two (1..512) = bitstrings executed together in one interleaved table. */
+int rgs_scan_workspace_bytes(const rgs_plan* plan, int32_t batch_tile, int32_t precision, size_t* bytes);
+
+/* Bitstring interface: f_q = U_q[x_q, :] (W/scan_oracle.py:26).
+ * unitaries: device complex128[n][2][2]; bits: device uint64[batch][2];
+ * out_value: device complex64[batch] (C64 precisions) or complex128[batch] (C128);
+ * out_logscale: device float64[batch]. */
+int rgs_scan_amplitudes(rgs_plan* plan, const double* unitaries, const uint64_t* bits, int64_t batch,
+                        int32_t precision, void* out_value, double* out_logscale, void* workspace,
+                        size_t workspace_bytes, int32_t batch_tile, void* stream);
+
+/* Contraction-vector interface (the GPUMixin._sweep(f, yfix) contract):
+ * fvec: device complex128[batch][n][2], f_q for every vertex of every item. */
+int rgs_scan_contract(rgs_plan* plan, const double* fvec, int64_t batch, int32_t precision,
+                      void* out_value, double* out_logscale, void* workspace, size_t workspace_bytes,
+                      int32_t batch_tile, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RGS_B200_H */

@@ -1,0 +1,17 @@
+"""B200-native graph-state probability and exact Born-sampling engine.
+
+Drop-in for the scan-contraction and conditional-sampler path of
+whyihaveyou/rgs70-classical-challenge.  Python host code calls hand-written
+sm_100a CUDA kernels in ``librgs_b200.so`` through the C ABI of
+``include/rgs_b200.h``; torch tensors are used only as device buffers.
+"""
+from . import _lib
+from .plan import ScanPlan, Step, make_plan, future_masks, rank_profile, byte_tables, kernel_combos, \
+    edges_from_graph
+from .scan_oracle import ScanEngine, ScanOracle, pack_bits, amplitudes_from, PRECISIONS
+from . import instances
+
+__all__ = [
+    "ScanPlan", "Step", "make_plan", "future_masks", "rank_profile", "byte_tables", "kernel_combos",
+    "edges_from_graph", "ScanEngine", "ScanOracle", "pack_bits", "amplitudes_from", "PRECISIONS",
+]

@@ -1,0 +1,179 @@
+// C ABI entry points (include/rgs_b200.h).  Thin wrappers: argument checks, error
+// recording, conversion between plain arrays and the C++ plan.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "common.hpp"
+#include "plan.hpp"
+#include "scan.hpp"
+
+struct rgs_plan {
+  rgs::Plan plan;
+};
+
+namespace rgs {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+const char* last_error() { return g_last_error.c_str(); }
+
+namespace {
+
+int read_graph(int32_t n, int32_t n_edges, const int32_t* edges, const int32_t* order, const uint8_t* fixed,
+               std::vector<std::pair<int, int>>& e, std::vector<int>& o, std::vector<uint8_t>& f) {
+  if (n < 1 || n > 128) return fail(RGS_ERR_ARG, "n must be in [1, 128]");
+  if (n_edges < 0 || (n_edges > 0 && !edges)) return fail(RGS_ERR_ARG, "bad edge list");
+  if (!order) return fail(RGS_ERR_ARG, "order is required");
+  e.resize(n_edges);
+  for (int i = 0; i < n_edges; ++i) e[i] = {edges[2 * i], edges[2 * i + 1]};
+  o.assign(order, order + n);
+  if (fixed) f.assign(fixed, fixed + n);
+  return RGS_OK;
+}
+
+void put128(uint64_t* dst, u128 x) {
+  dst[0] = (uint64_t)x;
+  dst[1] = (uint64_t)(x >> 64);
+}
+
+}  // namespace
+}  // namespace rgs
+
+using namespace rgs;
+
+extern "C" {
+
+const char* rgs_version(void) { return "rgs_b200 0.1 (sm_100a)"; }
+
+const char* rgs_last_error(void) { return rgs::last_error(); }
+
+int rgs_device_count(void) {
+  int c = 0;
+  if (cudaGetDeviceCount(&c) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return c;
+}
+
+int rgs_plan_compile(int32_t n, int32_t n_edges, const int32_t* edges, const int32_t* order, const uint8_t* fixed,
+                     rgs_plan** out_plan) {
+  if (!out_plan) return fail(RGS_ERR_ARG, "out_plan is NULL");
+  *out_plan = nullptr;
+  std::vector<std::pair<int, int>> e;
+  std::vector<int> o;
+  std::vector<uint8_t> f;
+  int rc = read_graph(n, n_edges, edges, order, fixed, e, o, f);
+  if (rc) return rc;
+  rgs_plan* p = new (std::nothrow) rgs_plan;
+  if (!p) return fail(RGS_ERR_OOM, "host allocation failed");
+  std::string err = compile_plan(n, e, o, f, p->plan);
+  if (!err.empty()) {
+    delete p;
+    return fail(RGS_ERR_ARG, err);
+  }
+  *out_plan = p;
+  return RGS_OK;
+}
+
+void rgs_plan_destroy(rgs_plan* plan) { delete plan; }
+
+int rgs_plan_info(const rgs_plan* plan, int32_t* n, int32_t* rmax, int32_t* executable) {
+  if (!plan) return fail(RGS_ERR_ARG, "plan is NULL");
+  if (n) *n = plan->plan.n;
+  if (rmax) *rmax = plan->plan.rmax;
+  if (executable) *executable = plan->plan.exec_ok ? 1 : 0;
+  return RGS_OK;
+}
+
+int rgs_plan_ranks(const rgs_plan* plan, int32_t* ranks) {
+  if (!plan || !ranks) return fail(RGS_ERR_ARG, "null argument");
+  for (int j = 0; j < plan->plan.n; ++j) ranks[j] = plan->plan.ranks[j];
+  return RGS_OK;
+}
+
+int rgs_plan_future_masks(const rgs_plan* plan, uint64_t* fut) {
+  if (!plan || !fut) return fail(RGS_ERR_ARG, "null argument");
+  for (int j = 0; j < plan->plan.n; ++j) put128(fut + 2 * j, plan->plan.future[j]);
+  return RGS_OK;
+}
+
+int rgs_plan_step(const rgs_plan* plan, int32_t j, int32_t* v, int32_t* is_free, int32_t* r_in, int32_t* r_out,
+                  uint64_t* beta, uint64_t* lcols, int32_t* n_kernel, uint64_t* kernel) {
+  if (!plan) return fail(RGS_ERR_ARG, "plan is NULL");
+  if (j < 0 || j >= plan->plan.n) return fail(RGS_ERR_ARG, "step index out of range");
+  const PlanStep& st = plan->plan.steps[j];
+  if (v) *v = st.v;
+  if (is_free) *is_free = st.free ? 1 : 0;
+  if (r_in) *r_in = st.r_in;
+  if (r_out) *r_out = st.r_out;
+  if (beta) put128(beta, st.beta);
+  if (lcols)
+    for (int k = 0; k < st.r_out; ++k) put128(lcols + 2 * k, st.lcols[k]);
+  if (n_kernel) *n_kernel = (int32_t)st.kernel.size();
+  if (kernel)
+    for (size_t k = 0; k < st.kernel.size(); ++k) put128(kernel + 2 * k, st.kernel[k]);
+  return RGS_OK;
+}
+
+int rgs_plan_step_tables(const rgs_plan* plan, int32_t j, uint64_t* tables, int32_t* nbytes) {
+  if (!plan) return fail(RGS_ERR_ARG, "plan is NULL");
+  if (j < 0 || j >= plan->plan.n) return fail(RGS_ERR_ARG, "step index out of range");
+  const PlanStep& st = plan->plan.steps[j];
+  std::vector<u128> t;
+  int nb = 0;
+  byte_tables(st.lcols, st.r_out, t, nb);
+  if (nbytes) *nbytes = nb;
+  if (tables)
+    for (size_t i = 0; i < t.size(); ++i) put128(tables + 2 * i, t[i]);
+  return RGS_OK;
+}
+
+int rgs_rank_profile(int32_t n, int32_t n_edges, const int32_t* edges, const int32_t* order, const uint8_t* fixed,
+                     int32_t* ranks) {
+  if (!ranks) return fail(RGS_ERR_ARG, "ranks is NULL");
+  std::vector<std::pair<int, int>> e;
+  std::vector<int> o;
+  std::vector<uint8_t> f;
+  int rc = read_graph(n, n_edges, edges, order, fixed, e, o, f);
+  if (rc) return rc;
+  std::vector<int> r;
+  std::string err = rank_profile(n, e, o, f, r);
+  if (!err.empty()) return fail(RGS_ERR_ARG, err);
+  for (int j = 0; j < n; ++j) ranks[j] = r[j];
+  return RGS_OK;
+}
+
+int rgs_scan_workspace_bytes(const rgs_plan* plan, int32_t batch_tile, int32_t precision, size_t* bytes) {
+  if (!plan || !bytes) return fail(RGS_ERR_ARG, "null argument");
+  ScanLayout L;
+  int rc = scan_layout(plan->plan, batch_tile, precision, L);
+  if (rc) return rc;
+  *bytes = L.total();
+  return RGS_OK;
+}
+
+int rgs_scan_amplitudes(rgs_plan* plan, const double* unitaries, const uint64_t* bits, int64_t batch,
+                        int32_t precision, void* out_value, double* out_logscale, void* workspace,
+                        size_t workspace_bytes, int32_t batch_tile, void* stream) {
+  if (!plan) return fail(RGS_ERR_ARG, "plan is NULL");
+  if (!unitaries || !bits) return fail(RGS_ERR_ARG, "unitaries and bits are required");
+  return scan_run(plan->plan, unitaries, (const unsigned long long*)bits, nullptr, batch, precision, out_value,
+                  out_logscale, workspace, workspace_bytes, batch_tile, (cudaStream_t)stream, nullptr);
+}
+
+int rgs_scan_contract(rgs_plan* plan, const double* fvec, int64_t batch, int32_t precision, void* out_value,
+                      double* out_logscale, void* workspace, size_t workspace_bytes, int32_t batch_tile,
+                      void* stream) {
+  if (!plan) return fail(RGS_ERR_ARG, "plan is NULL");
+  if (!fvec) return fail(RGS_ERR_ARG, "fvec is required");
+  return scan_run(plan->plan, nullptr, nullptr, fvec, batch, precision, out_value, out_logscale, workspace,
+                  workspace_bytes, batch_tile, (cudaStream_t)stream, nullptr);
+}
+
+}  // extern "C"

@@ -1,0 +1,395 @@
+// Scan executor: batched graph-state amplitudes on sm_100a.
+//
+// Replaces the per-step CuPy kernel and host loop of whyihaveyou/rgs70-classical-challenge
+// (W/upstream_scan/gpu_kernel.py:59-170 and gpu_kernel_fp64.py:24-135):
+//  * a batch tile of Bt bitstrings runs as one interleaved table E[c][b], so every
+//    gather is a contiguous Bt-item row (128-bit loads);
+//  * outputs c' and c'^t (t = image of the y unit vector) read the same inputs, so a
+//    thread produces both and each input entry is read once per step (the reference
+//    reads every input twice and relies on caches for the second read);
+//  * the power-of-two renormalisation is derived on the device from the previous
+//    step's maximum, so a sweep is a fixed launch sequence with no host round trip.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+
+#include "common.hpp"
+#include "plan.hpp"
+#include "scan.hpp"
+#include "scan_device.cuh"
+
+namespace rgs {
+
+Plan::~Plan() {
+  int prev = -1;
+  cudaGetDevice(&prev);
+  for (auto& d : device_copies) {
+    if (d.device < 0) continue;
+    cudaSetDevice(d.device);
+    if (d.steps) cudaFree(d.steps);
+    if (d.tables) cudaFree(d.tables);
+    if (d.verts) cudaFree(d.verts);
+  }
+  if (prev >= 0) cudaSetDevice(prev);
+}
+
+int sm_count(int device) {
+  static int cache[64] = {0};
+  if (device < 0 || device >= 64) return 148;
+  if (!cache[device]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || v <= 0) v = 148;
+    cache[device] = v;
+  }
+  return cache[device];
+}
+
+// The library carries its own CUDA runtime, whose current device is independent of
+// the caller's runtime; the device is taken from a caller-owned device pointer.
+int bind_device_of(const void* p, int* device) {
+  cudaPointerAttributes a;
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(RGS_ERR_ARG, std::string("pointer is not CUDA memory: ") + cudaGetErrorString(e));
+  }
+  if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)
+    return fail(RGS_ERR_ARG, "workspace/output must be device memory");
+  RGS_CUDA_TRY(cudaSetDevice(a.device));
+  *device = a.device;
+  return RGS_OK;
+}
+
+static std::mutex g_upload_mutex;
+
+int plan_device_copy(Plan& plan, int device, const Plan::DeviceCopy** out) {
+  std::lock_guard<std::mutex> lock(g_upload_mutex);
+  for (auto& d : plan.device_copies)
+    if (d.device == device) {
+      *out = &d;
+      return RGS_OK;
+    }
+  if (!plan.exec_ok) return fail(RGS_ERR_UNSUPPORTED, plan.exec_reason);
+  Plan::DeviceCopy d;
+  d.device = device;
+  std::vector<DevVert> verts(plan.n);
+  for (int j = 0; j < plan.n; ++j) {
+    verts[j].fut_lo = (unsigned long long)plan.future[j];
+    verts[j].fut_hi = (unsigned long long)(plan.future[j] >> 64);
+    verts[j].v = plan.steps[j].v;
+    verts[j].fixed = plan.steps[j].free ? 0 : 1;
+  }
+  const size_t tb = std::max<size_t>(1, plan.tables.size()) * sizeof(unsigned long long);
+  RGS_CUDA_TRY(cudaMalloc(&d.steps, sizeof(DevStep) * plan.n));
+  RGS_CUDA_TRY(cudaMalloc(&d.tables, tb));
+  RGS_CUDA_TRY(cudaMalloc(&d.verts, sizeof(DevVert) * plan.n));
+  RGS_CUDA_TRY(cudaMemcpy(d.steps, plan.dev.data(), sizeof(DevStep) * plan.n, cudaMemcpyHostToDevice));
+  if (!plan.tables.empty())
+    RGS_CUDA_TRY(cudaMemcpy(d.tables, plan.tables.data(), plan.tables.size() * sizeof(unsigned long long),
+                            cudaMemcpyHostToDevice));
+  RGS_CUDA_TRY(cudaMemcpy(d.verts, verts.data(), sizeof(DevVert) * plan.n, cudaMemcpyHostToDevice));
+  plan.device_copies.push_back(d);
+  *out = &plan.device_copies.back();
+  return RGS_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Weights: W[j][b] = (f_v(0), f_v(1)) of item b at position j, and for plans with fixed
+// vertices the flags y | ov << 1 (the affine syndrome offset of scan_plan.py:167-172).
+__global__ void scan_weights_kernel(const DevVert* __restrict__ verts, int n, const double2* __restrict__ U,
+                                    const u64* __restrict__ bits, const double2* __restrict__ fvec,
+                                    long long first, int count, int Bt, double4* __restrict__ W,
+                                    unsigned char* __restrict__ F) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= Bt) return;
+  if (b >= count) {
+    for (int j = 0; j < n; ++j) {
+      W[(size_t)j * Bt + b] = make_double4(0.0, 0.0, 0.0, 0.0);
+      if (F) F[(size_t)j * Bt + b] = 0;
+    }
+    return;
+  }
+  const long long item = first + b;
+  u64 lo = 0, hi = 0;
+  if (bits) {
+    lo = bits[2 * item];
+    hi = bits[2 * item + 1];
+  }
+  u64 olo = 0, ohi = 0;
+  for (int j = 0; j < n; ++j) {
+    const DevVert vt = verts[j];
+    double2 f0, f1;
+    if (fvec) {
+      f0 = fvec[((size_t)item * n + vt.v) * 2 + 0];
+      f1 = fvec[((size_t)item * n + vt.v) * 2 + 1];
+    } else {
+      const int x = (int)((vt.v < 64 ? (lo >> vt.v) : (hi >> (vt.v - 64))) & 1ull);
+      f0 = U[(vt.v * 2 + x) * 2 + 0];
+      f1 = U[(vt.v * 2 + x) * 2 + 1];
+    }
+    const int ov = (int)((j < 64 ? (olo >> j) : (ohi >> (j - 64))) & 1ull);
+    if (j < 64)
+      olo &= ~(1ull << j);
+    else
+      ohi &= ~(1ull << (j - 64));
+    int y = 0;
+    if (vt.fixed) {
+      y = hypot(f0.x, f0.y) > 1e-12 ? 0 : 1;
+      if (y) {
+        olo ^= vt.fut_lo;
+        ohi ^= vt.fut_hi;
+      }
+    }
+    W[(size_t)j * Bt + b] = make_double4(f0.x, f0.y, f1.x, f1.y);
+    if (F) F[(size_t)j * Bt + b] = (unsigned char)(y | (ov << 1));
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// One scan position over a batch tile.  Grid-stride over items; a thread keeps its V
+// items (lane) for the whole launch, so weights and scales are set up once.
+template <typename S, typename M, int V, int MODE>
+__global__ void __launch_bounds__(256) scan_step_kernel(const S* __restrict__ Ein, S* __restrict__ Eout,
+                                                        const __grid_constant__ DevStep st,
+                                                        const u64* __restrict__ T, const double4* __restrict__ W,
+                                                        const unsigned char* __restrict__ F,
+                                                        const u64* __restrict__ maxprev,
+                                                        u64* __restrict__ maxcur, int lbt, int unit_input) {
+  __shared__ u64 smax[512];
+  const int Bt = 1 << lbt;
+  const int llpr = lbt - (V == 2 ? 1 : 0);  // log2 lanes per row
+  const u64 tid = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = (int)(tid & ((1ull << llpr) - 1ull));
+  const int b0 = lane * V;
+
+  for (int i = threadIdx.x; i < Bt; i += blockDim.x) smax[i] = 0;
+
+  StepWeights<M, V> w;
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    const int b = b0 + v;
+    const double m2 = maxprev ? max_value<S>(maxprev[b]) : 1.0;
+    const double s = ldexp(1.0, -scale_exponent(m2));
+    const double4 f = W[b];
+    w.w0[v].re = (M)(f.x * s);
+    w.w0[v].im = (M)(f.y * s);
+    w.w1[v].re = (M)(f.z * s);
+    w.w1[v].im = (M)(f.w * s);
+    const int fl = F ? F[b] : 0;
+    w.y[v] = fl & 1;
+    w.ov[v] = (fl >> 1) & 1;
+  }
+  __syncthreads();
+
+  const u64 items = (MODE == MODE_PAIR) ? (1ull << (st.r_out - 1)) : (1ull << st.r_out);
+  const u64 stride = ((u64)gridDim.x * blockDim.x) >> llpr;
+  S mx[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) mx[v] = (S)0;
+
+  for (u64 item = tid >> llpr; item < items; item += stride) {
+    u64 ca, cb;
+    Cx<M> oa[V], ob[V];
+    step_item<S, M, V, MODE, RowIO<S, V>>(Ein, st, T, w, item, lbt, b0, unit_input != 0, ca, cb, oa, ob);
+    S ra[V], ia[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      ra[v] = (S)oa[v].re;
+      ia[v] = (S)oa[v].im;
+      mx[v] = fmax(mx[v], ra[v] * ra[v] + ia[v] * ia[v]);
+    }
+    RowIO<S, V>::store(Eout, (ca << lbt) + (u64)b0, ra, ia);
+    if (MODE == MODE_PAIR) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        ra[v] = (S)ob[v].re;
+        ia[v] = (S)ob[v].im;
+        mx[v] = fmax(mx[v], ra[v] * ra[v] + ia[v] * ia[v]);
+      }
+      RowIO<S, V>::store(Eout, (cb << lbt) + (u64)b0, ra, ia);
+    }
+  }
+
+  // Maximum |E|^2 per item: lanes of one warp that share items first, then shared
+  // memory, then one global atomic per item per block (gpu_kernel.py:98-101).
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    u64 bitsv = max_bits<S>(mx[v]);
+    for (int off = 16; off >= (1 << llpr) && off >= 1; off >>= 1) {
+      const u64 o = __shfl_xor_sync(0xffffffffu, bitsv, off);
+      bitsv = bitsv > o ? bitsv : o;
+    }
+    if ((threadIdx.x & 31) < (1 << llpr) && bitsv) atomicMax(&smax[b0 + v], bitsv);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < Bt; i += blockDim.x)
+    if (smax[i]) atomicMax(&maxcur[i], smax[i]);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Final value and log-scale per item (gpu_kernel.py:126-170): value = E[0], logscale =
+// ln2 * sum_j e_j, with e_0 = 1 and e_j from the maximum after step j-1.  An all-zero
+// table ends the sum as in the reference (value 0); a non-finite maximum yields NaN.
+template <typename S>
+__global__ void scan_finalize_kernel(const S* __restrict__ E, const u64* __restrict__ maxbuf, int n, int Bt,
+                                     int count, S* __restrict__ out_value, double* __restrict__ out_logscale) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= count) return;
+  long long esum = 0;
+  bool zero = false, bad = false;
+  double m2prev = 1.0;
+  for (int j = 0; j < n; ++j) {
+    esum += scale_exponent(m2prev);
+    const double m2 = max_value<S>(maxbuf[(size_t)j * Bt + b]);
+    if (!isfinite(m2)) {
+      bad = true;
+      break;
+    }
+    if (!(m2 > 0.0)) {
+      zero = true;
+      break;
+    }
+    m2prev = m2;
+  }
+  S re = E[2 * (size_t)b], im = E[2 * (size_t)b + 1];
+  if (zero) re = im = (S)0;
+  if (bad) re = im = (S)NAN;
+  out_value[2 * (size_t)b] = re;
+  out_value[2 * (size_t)b + 1] = im;
+  out_logscale[b] = (double)esum * 0.69314718055994530942;
+}
+
+// ------------------------------------------------------------------------------------------------
+size_t ScanLayout::total() const { return off_max + bytes_max; }
+
+int scan_layout(const Plan& plan, int Bt, int precision, ScanLayout& L) {
+  if (Bt < 1 || Bt > 512 || (Bt & (Bt - 1))) return fail(RGS_ERR_ARG, "batch_tile must be a power of two in [1, 512]");
+  if (precision < RGS_PREC_C64 || precision > RGS_PREC_C128) return fail(RGS_ERR_ARG, "unknown precision");
+  if (!plan.exec_ok) return fail(RGS_ERR_UNSUPPORTED, plan.exec_reason);
+  const size_t esize = precision == RGS_PREC_C128 ? 16 : 8;
+  // A row of Bt items must be covered by at most one 256-thread block (16 bytes per thread).
+  if ((size_t)Bt * esize > 256 * 16) return fail(RGS_ERR_ARG, "batch_tile too large for complex128 (max 256)");
+  L.Bt = Bt;
+  L.esize = esize;
+  L.bytes_buf = align_up(((size_t)1 << plan.rmax) * (size_t)Bt * esize, 256);
+  L.bytes_w = align_up((size_t)plan.n * Bt * sizeof(double4), 256);
+  L.bytes_f = align_up((size_t)plan.n * Bt, 256);
+  L.bytes_max = align_up((size_t)plan.n * Bt * sizeof(u64), 256);
+  L.off_buf0 = 0;
+  L.off_buf1 = L.bytes_buf;
+  L.off_w = 2 * L.bytes_buf;
+  L.off_f = L.off_w + L.bytes_w;
+  L.off_max = L.off_f + L.bytes_f;
+  return RGS_OK;
+}
+
+namespace {
+
+template <typename S, typename M, int V>
+cudaError_t launch_step_v(int mode, dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevStep& st,
+                          const u64* T, const double4* W, const unsigned char* F, const u64* mp, u64* mc, int lbt,
+                          int unit) {
+  const S* in = (const S*)Ein;
+  S* out = (S*)Eout;
+  switch (mode) {
+    case MODE_PAIR:
+      scan_step_kernel<S, M, V, MODE_PAIR><<<grid, 256, 0, s>>>(in, out, st, T, W, F, mp, mc, lbt, unit);
+      break;
+    case MODE_MERGE:
+      scan_step_kernel<S, M, V, MODE_MERGE><<<grid, 256, 0, s>>>(in, out, st, T, W, F, mp, mc, lbt, unit);
+      break;
+    default:
+      scan_step_kernel<S, M, V, MODE_FIXED><<<grid, 256, 0, s>>>(in, out, st, T, W, F, mp, mc, lbt, unit);
+      break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_step(int precision, int V, int mode, dim3 grid, cudaStream_t s, const void* Ein, void* Eout,
+                        const DevStep& st, const u64* T, const double4* W, const unsigned char* F, const u64* mp,
+                        u64* mc, int lbt, int unit) {
+  if (precision == RGS_PREC_C128) return launch_step_v<double, double, 1>(mode, grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+  if (precision == RGS_PREC_C64) {
+    if (V == 2) return launch_step_v<float, double, 2>(mode, grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+    return launch_step_v<float, double, 1>(mode, grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+  }
+  if (V == 2) return launch_step_v<float, float, 2>(mode, grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+  return launch_step_v<float, float, 1>(mode, grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+}
+
+bool plan_has_fixed(const Plan& p) {
+  for (auto& st : p.steps)
+    if (!st.free) return true;
+  return false;
+}
+
+}  // namespace
+
+int scan_run(Plan& plan, const double* U, const u64* bits, const double* fvec, long long batch, int precision,
+             void* out_value, double* out_logscale, void* workspace, size_t ws_bytes, int Bt, cudaStream_t stream,
+             ScanStats* stats) {
+  if (batch < 0) return fail(RGS_ERR_ARG, "batch must be >= 0");
+  if (batch == 0) return RGS_OK;
+  if (!out_value || !out_logscale || !workspace) return fail(RGS_ERR_ARG, "null output or workspace pointer");
+  if (!fvec && (!U || !bits)) return fail(RGS_ERR_ARG, "need unitaries and bits, or contraction vectors");
+  ScanLayout L;
+  int rc = scan_layout(plan, Bt, precision, L);
+  if (rc) return rc;
+  if (ws_bytes < L.total()) return fail(RGS_ERR_OOM, "workspace smaller than rgs_scan_workspace_bytes()");
+  if (((uintptr_t)workspace & 255) != 0) return fail(RGS_ERR_ARG, "workspace must be 256-byte aligned");
+  int device = 0;
+  rc = bind_device_of(workspace, &device);
+  if (rc) return rc;
+  const Plan::DeviceCopy* dc = nullptr;
+  rc = plan_device_copy(plan, device, &dc);
+  if (rc) return rc;
+
+  char* ws = (char*)workspace;
+  void* buf[2] = {ws + L.off_buf0, ws + L.off_buf1};
+  double4* W = (double4*)(ws + L.off_w);
+  unsigned char* F = plan_has_fixed(plan) ? (unsigned char*)(ws + L.off_f) : nullptr;
+  u64* maxbuf = (u64*)(ws + L.off_max);
+  const u64* tables = (const u64*)dc->tables;
+  const int lbt = __builtin_ctz((unsigned)Bt);
+  const int V = (precision != RGS_PREC_C128 && Bt >= 2) ? 2 : 1;
+  const int lpr = Bt / V;
+  const int sms = sm_count(device);
+  const long long max_blocks = (long long)sms * 8;
+  const size_t esize = L.esize;
+  long long launches = 0;
+
+  for (long long first = 0; first < batch; first += Bt) {
+    const int count = (int)std::min<long long>(Bt, batch - first);
+    scan_weights_kernel<<<(Bt + 127) / 128, 128, 0, stream>>>((const DevVert*)dc->verts, plan.n, (const double2*)U,
+                                                              bits, (const double2*)fvec, first, count, Bt, W, F);
+    RGS_CUDA_TRY(cudaGetLastError());
+    RGS_CUDA_TRY(cudaMemsetAsync(maxbuf, 0, (size_t)plan.n * Bt * sizeof(u64), stream));
+    launches += 1;
+    for (int j = 0; j < plan.n; ++j) {
+      const DevStep& st = plan.dev[j];
+      const u64 items = st.mode == MODE_PAIR ? (1ull << (st.r_out - 1)) : (1ull << st.r_out);
+      const long long threads = (long long)items * lpr;
+      const long long blocks = std::max<long long>(1, std::min<long long>((threads + 255) / 256, max_blocks));
+      RGS_CUDA_TRY(launch_step(precision, V, st.mode, dim3((unsigned)blocks), stream, buf[j & 1], buf[(j + 1) & 1], st,
+                               tables + st.table_off, W + (size_t)j * Bt, F ? F + (size_t)j * Bt : nullptr,
+                               j ? maxbuf + (size_t)(j - 1) * Bt : nullptr, maxbuf + (size_t)j * Bt, lbt, j == 0));
+      launches += 1;
+    }
+    const void* fin = buf[plan.n & 1];
+    if (precision == RGS_PREC_C128)
+      scan_finalize_kernel<double><<<(count + 127) / 128, 128, 0, stream>>>(
+          (const double*)fin, maxbuf, plan.n, Bt, count, (double*)out_value + 2 * first, out_logscale + first);
+    else
+      scan_finalize_kernel<float><<<(count + 127) / 128, 128, 0, stream>>>(
+          (const float*)fin, maxbuf, plan.n, Bt, count, (float*)out_value + 2 * first, out_logscale + first);
+    RGS_CUDA_TRY(cudaGetLastError());
+    launches += 1;
+  }
+  (void)esize;
+  if (stats) stats->launches = launches;
+  return RGS_OK;
+}
+
+}  // namespace rgs

@@ -1,0 +1,39 @@
+// Host interface of the scan executor (scan.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+#include "plan.hpp"
+
+namespace rgs {
+
+// Workspace partition for one batch tile: two ping-pong tables, weights, flags and
+// per-step maxima (all offsets 256-byte aligned).
+struct ScanLayout {
+  int Bt = 1;
+  size_t esize = 8;
+  size_t bytes_buf = 0, bytes_w = 0, bytes_f = 0, bytes_max = 0;
+  size_t off_buf0 = 0, off_buf1 = 0, off_w = 0, off_f = 0, off_max = 0;
+  size_t total() const;
+};
+
+struct ScanStats {
+  long long launches = 0;
+};
+
+int scan_layout(const Plan& plan, int Bt, int precision, ScanLayout& L);
+
+// Makes the device owning `p` current for this library's runtime and returns it.
+int bind_device_of(const void* p, int* device);
+
+// Uploads (once per device) the plan's step records, byte tables and vertex records.
+int plan_device_copy(Plan& plan, int device, const Plan::DeviceCopy** out);
+
+// Runs the sweep for `batch` items: either bits (+ unitaries) or explicit contraction
+// vectors fvec.  All work is queued on `stream`.
+int scan_run(Plan& plan, const double* U, const unsigned long long* bits, const double* fvec, long long batch,
+             int precision, void* out_value, double* out_logscale, void* workspace, size_t ws_bytes, int Bt,
+             cudaStream_t stream, ScanStats* stats);
+
+}  // namespace rgs
