@@ -162,6 +162,7 @@ int rgs_scan_amplitudes(rgs_plan* plan, const double* unitaries, const uint64_t*
                         int32_t precision, void* out_value, double* out_logscale, void* workspace,
                         size_t workspace_bytes, int32_t batch_tile, void* stream) {
   if (!plan) return fail(RGS_ERR_ARG, "plan is NULL");
+  if (batch == 0) return RGS_OK;
   if (!unitaries || !bits) return fail(RGS_ERR_ARG, "unitaries and bits are required");
   return scan_run(plan->plan, unitaries, (const unsigned long long*)bits, nullptr, batch, precision, out_value,
                   out_logscale, workspace, workspace_bytes, batch_tile, (cudaStream_t)stream, nullptr);
@@ -171,6 +172,7 @@ int rgs_scan_contract(rgs_plan* plan, const double* fvec, int64_t batch, int32_t
                       double* out_logscale, void* workspace, size_t workspace_bytes, int32_t batch_tile,
                       void* stream) {
   if (!plan) return fail(RGS_ERR_ARG, "plan is NULL");
+  if (batch == 0) return RGS_OK;
   if (!fvec) return fail(RGS_ERR_ARG, "fvec is required");
   return scan_run(plan->plan, nullptr, nullptr, fvec, batch, precision, out_value, out_logscale, workspace,
                   workspace_bytes, batch_tile, (cudaStream_t)stream, nullptr);
