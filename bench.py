@@ -191,16 +191,21 @@ def run_ours(args, rank, world, local_rank):
     rng = np.random.default_rng(BITS_SEED + rank)
     bits = pkg.instances.uniform_bits(BATCH, N_QUBITS, rng)
     packed = pkg.pack_bits(bits, N_QUBITS)
-    eng64 = pkg.ScanEngine(plan, inst.u, device=device, precision="c64", batch_tile=512)
-    eng128 = pkg.ScanEngine(plan, inst.u, device=device, precision="c128", batch_tile=256)
+    tile64 = min(args.tile64, 1 << max(0, (BATCH - 1).bit_length()))
+    tile128 = min(args.tile128, 1 << max(0, (BATCH - 1).bit_length()))
+    use64, use128 = args.only in ("both", "c64"), args.only in ("both", "c128")
+    eng64 = pkg.ScanEngine(plan, inst.u, device=device, precision="c64", batch_tile=tile64) if use64 else None
+    eng128 = pkg.ScanEngine(plan, inst.u, device=device, precision="c128", batch_tile=tile128) if use128 else None
     d_bits = torch.from_numpy(packed.view(np.int64)).to(device)
-    v64, l64 = eng64.out_tensors(BATCH)
-    v128, l128 = eng128.out_tensors(BATCH)
+    v64, l64 = eng64.out_tensors(BATCH) if use64 else (None, None)
+    v128, l128 = eng128.out_tensors(BATCH) if use128 else (None, None)
     stream = torch.cuda.current_stream(device)
 
     def device_step():
-        eng64.run_bits(d_bits, v64, l64, stream=stream)
-        eng128.run_bits(d_bits, v128, l128, stream=stream)
+        if use64:
+            eng64.run_bits(d_bits, v64, l64, stream=stream)
+        if use128:
+            eng128.run_bits(d_bits, v128, l128, stream=stream)
 
     def barrier():
         if world > 1:
@@ -230,14 +235,23 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize(device)
     with ClockSampler(local_rank) as clocks:
         t_step = timed(device_step, args.steps)
-    # Split of the step, and the FP64 recheck error.
-    t64 = timed(lambda: eng64.run_bits(d_bits, v64, l64, stream=stream), args.steps)
-    t128 = timed(lambda: eng128.run_bits(d_bits, v128, l128, stream=stream), args.steps)
-    p64 = np.abs(pkg.amplitudes_from(v64.cpu().numpy(), l64.cpu().numpy(), N_QUBITS)) ** 2
-    p128 = np.abs(pkg.amplitudes_from(v128.cpu().numpy(), l128.cpu().numpy(), N_QUBITS)) ** 2
-    if not (np.all(np.isfinite(p64)) and np.all(np.isfinite(p128))):
-        raise ArithmeticError("non-finite probability in the benchmark run")
-    recheck_err = float(np.max(np.abs(p64 - p128) / p128))
+    # Split of the step, and the FP64 recheck error (per result: max and quantiles).
+    t64 = timed(lambda: eng64.run_bits(d_bits, v64, l64, stream=stream), args.steps) if use64 else None
+    t128 = timed(lambda: eng128.run_bits(d_bits, v128, l128, stream=stream), args.steps) if use128 else None
+    recheck = None
+    p128 = None
+    if use64 and use128:
+        p64 = np.abs(pkg.amplitudes_from(v64.cpu().numpy(), l64.cpu().numpy(), N_QUBITS)) ** 2
+        p128 = np.abs(pkg.amplitudes_from(v128.cpu().numpy(), l128.cpu().numpy(), N_QUBITS)) ** 2
+        if not (np.all(np.isfinite(p64)) and np.all(np.isfinite(p128))):
+            raise ArithmeticError("non-finite probability in the benchmark run")
+        rel = np.abs(p64 - p128) / p128
+        scaled = np.abs(p64 - p128) * 2.0 ** N_QUBITS
+        recheck = {"max_prob_rel_err": float(rel.max()), "median_prob_rel_err": float(np.median(rel)),
+                   "p999_prob_rel_err": float(np.quantile(rel, 0.999)),
+                   "frac_above_1e-4": float(np.mean(rel > 1e-4)),
+                   "max_rel_err_p_ge_0.01_over_2^n": float(rel[p128 * 2.0 ** N_QUBITS >= 0.01].max()),
+                   "max_abs_err_times_2^n": float(scaled.max())}
 
     # End to end through the public API: pinned host bits in, host probabilities out.
     h_bits = torch.from_numpy(packed.view(np.int64)).pin_memory()
@@ -249,20 +263,24 @@ def run_ours(args, rank, world, local_rank):
     def e2e_step():
         d_bits.copy_(h_bits, non_blocking=True)
         device_step()
-        h_v64.copy_(v64, non_blocking=True)
-        h_l64.copy_(l64, non_blocking=True)
-        h_v128.copy_(v128, non_blocking=True)
-        h_l128.copy_(l128, non_blocking=True)
+        if use64:
+            h_v64.copy_(v64, non_blocking=True)
+            h_l64.copy_(l64, non_blocking=True)
+        if use128:
+            h_v128.copy_(v128, non_blocking=True)
+            h_l128.copy_(l128, non_blocking=True)
 
-    for _ in range(max(1, args.warmup // 2)):
-        e2e_step()
-    t_e2e = timed(e2e_step, args.steps)
+    t_e2e = None
+    if not args.no_e2e:
+        for _ in range(max(1, args.warmup // 2)):
+            e2e_step()
+        t_e2e = timed(e2e_step, args.steps)
     h2d = packed.nbytes
-    d2h = BATCH * (8 + 8 + 16 + 8)
+    d2h = BATCH * ((8 + 8 if use64 else 0) + (16 + 8 if use128 else 0))
 
     # Roofline of the scan-step kernels (dominant: they are all but three launches per tile).
-    b64 = step_bytes(inst.ranks, 8) * BATCH
-    b128 = step_bytes(inst.ranks, 16) * BATCH
+    b64 = step_bytes(inst.ranks, 8) * BATCH if use64 else 0
+    b128 = step_bytes(inst.ranks, 16) * BATCH if use128 else 0
     peaks_path = ROOT / "MEASURED_PEAKS.json"
     peak, peak_src = 6650.0, "fallback"
     if peaks_path.exists():
@@ -270,8 +288,8 @@ def run_ours(args, rank, world, local_rank):
     achieved = (b64 + b128) / (t_step / args.steps) / 1e9
     traffic_path = ROOT / "profiles" / "scan_step_traffic.json"
     traffic = json.loads(traffic_path.read_text()).get("dram_bytes_per_step") if traffic_path.exists() else None
-    groups64 = math.ceil(BATCH / 512)
-    groups128 = math.ceil(BATCH / 256)
+    groups64 = math.ceil(BATCH / tile64) if use64 else 0
+    groups128 = math.ceil(BATCH / tile128) if use128 else 0
     launches = args.steps * ((groups64 + groups128) * (N_QUBITS + 2))
 
     line = None
@@ -283,8 +301,8 @@ def run_ours(args, rank, world, local_rank):
                    "sample": f"{2 * cores} amplitudes (complex128 NumPy sweep restated from the reference) "
                              f"on {cores} spawned processes"}
             p_cpu = np.abs(cpu_amps) ** 2
-            recheck_cpu = float(np.max(np.abs(p128[:len(p_cpu)] - p_cpu) / p_cpu))
-            cpu["parity_max_rel_err_vs_fp64"] = recheck_cpu
+            if p128 is not None:
+                cpu["parity_max_rel_err_vs_fp64"] = float(np.max(np.abs(p128[:len(p_cpu)] - p_cpu) / p_cpu))
         value = world * BATCH * args.steps / t_step
         line = {
             "metric": "amplitudes_per_s (p(x), n=40 3-regular, complex64 + FP64 recheck)",
@@ -295,18 +313,19 @@ def run_ours(args, rank, world, local_rank):
             "config": {"workload": "single-instance throughput: n=40 random 3-regular, Haar SU(2), "
                                    "65536 uniform 40-bit strings, complex64 + FP64 recheck of every result",
                        "instance": inst.name, "rmax": inst.rmax, "sum_states": inst.sum_states,
-                       "batch_per_gpu": BATCH, "batch_tile": {"c64": 512, "c128": 256},
+                       "batch_per_gpu": BATCH, "batch_tile": {"c64": tile64, "c128": tile128},
+                       "precisions": args.only,
                        "l2": "inputs larger than L2 (c64 tables 2 x 4 GiB, c128 2 x 4 GiB)",
                        "parallelism": f"replicas x{world}"},
-            "split": {"c64_amplitudes_per_s": world * BATCH * args.steps / t64,
-                      "c128_amplitudes_per_s": world * BATCH * args.steps / t128,
-                      "fp64_recheck_max_prob_rel_err": recheck_err},
+            "split": {"c64_amplitudes_per_s": world * BATCH * args.steps / t64 if t64 else None,
+                      "c128_amplitudes_per_s": world * BATCH * args.steps / t128 if t128 else None},
+            "fp64_recheck": recheck,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
                          "algorithmic_bytes_per_step": b64 + b128,
                          "reference_model_bytes_per_step": (reference_bytes(inst.ranks, 8)
                                                             + reference_bytes(inst.ranks, 16)) * BATCH},
-            "e2e": {"value": world * BATCH * args.steps / t_e2e, "unit": "amplitudes/s",
+            "e2e": {"value": world * BATCH * args.steps / t_e2e if t_e2e else None, "unit": "amplitudes/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
@@ -328,6 +347,11 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--batch", type=int, default=BATCH, help="bitstrings per GPU per step (profiling runs)")
+    ap.add_argument("--only", choices=["both", "c64", "c128"], default="both",
+                    help="run only one precision (profiling runs)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--tile64", type=int, default=512)
+    ap.add_argument("--tile128", type=int, default=256)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus if args.gpus == 1 else 1))
