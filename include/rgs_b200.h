@@ -105,6 +105,21 @@ int rgs_scan_contract(rgs_plan* plan, const double* fvec, int64_t batch, int32_t
                       void* out_value, double* out_logscale, void* workspace, size_t workspace_bytes,
                       int32_t batch_tile, void* stream);
 
+/* ---------------------------------------------------------------- allocation-free scan
+ * No counterpart in the reference.  Same result as rgs_scan_amplitudes, for callers
+ * that cannot allocate device memory at call time (host callbacks, hosts that give
+ * the library a fixed memory budget, integrations whose allocator must own every
+ * byte): no workspace argument, and no cudaMalloc/cudaFree or allocating library
+ * call.  All scratch lives in one static device array of RGS_NOALLOC_SCRATCH_BYTES
+ * (64 MiB) per GPU, held from library load until process exit; plans whose scratch
+ * does not fit (complex64 rank above about 21) are rejected with RGS_ERR_OOM.  The
+ * first call on a device looks up the array's address (make it before any stream
+ * capture).  Calls share the array: calls that overlap on the GPU race, so serialise
+ * them.  out_value: complex64[batch] or complex128[batch] (RGS_PREC_C128). */
+#define RGS_NOALLOC_SCRATCH_BYTES (64ull << 20)
+int rgs_scan_amplitudes_noalloc(rgs_plan* plan, const double* unitaries, const uint64_t* bits, int64_t batch,
+                                int32_t precision, void* out_value, double* out_logscale, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

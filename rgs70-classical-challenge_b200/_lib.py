@@ -64,6 +64,8 @@ SIGNATURES = {
                                            c_void_p]),
     "rgs_scan_contract": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int64, ctypes.c_int32, c_void_p,
                                          c_void_p, c_void_p, ctypes.c_size_t, ctypes.c_int32, c_void_p]),
+    "rgs_scan_amplitudes_noalloc": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_int64, ctypes.c_int32,
+                                                   c_void_p, c_void_p, c_void_p]),
 }
 
 _lib = None

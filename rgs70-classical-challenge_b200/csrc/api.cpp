@@ -11,10 +11,6 @@
 #include "plan.hpp"
 #include "scan.hpp"
 
-struct rgs_plan {
-  rgs::Plan plan;
-};
-
 namespace rgs {
 
 static thread_local std::string g_last_error;

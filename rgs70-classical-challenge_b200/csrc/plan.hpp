@@ -104,3 +104,8 @@ void byte_tables(const std::vector<u128>& cols, int nbits, std::vector<u128>& ou
 std::vector<u128> kernel_combos(const std::vector<u128>& kernel);
 
 }  // namespace rgs
+
+// Opaque handle of the C ABI (include/rgs_b200.h).
+struct rgs_plan {
+  rgs::Plan plan;
+};

@@ -392,4 +392,36 @@ int scan_run(Plan& plan, const double* U, const u64* bits, const double* fvec, l
   return RGS_OK;
 }
 
+// ------------------------------------------------------------------------------------------------
+cudaError_t scan_launch_weights(const DevVert* verts, int n, const double* U, const u64* bits, const double* fvec,
+                                long long first, int count, int Bt, void* W, unsigned char* F, cudaStream_t stream) {
+  scan_weights_kernel<<<(Bt + 127) / 128, 128, 0, stream>>>(verts, n, (const double2*)U, bits, (const double2*)fvec,
+                                                            first, count, Bt, (double4*)W, F);
+  return cudaGetLastError();
+}
+
+cudaError_t scan_launch_step(int precision, int Bt, int device, const DevStep& st, const void* Ein, void* Eout,
+                             const u64* T, const void* W, const unsigned char* F, const u64* maxprev, u64* maxcur,
+                             bool unit_input, cudaStream_t stream) {
+  const int lbt = __builtin_ctz((unsigned)Bt);
+  const int V = (precision != RGS_PREC_C128 && Bt >= 2) ? 2 : 1;
+  const u64 items = st.mode == MODE_PAIR ? (1ull << (st.r_out - 1)) : (1ull << st.r_out);
+  const long long threads = (long long)items * (Bt / V);
+  const long long max_blocks = (long long)sm_count(device) * 8;
+  const long long blocks = std::max<long long>(1, std::min<long long>((threads + 255) / 256, max_blocks));
+  return launch_step(precision, V, st.mode, dim3((unsigned)blocks), stream, Ein, Eout, st, T, (const double4*)W, F,
+                     maxprev, maxcur, lbt, unit_input ? 1 : 0);
+}
+
+cudaError_t scan_launch_finalize(int precision, const void* E, const u64* maxbuf, int n, int Bt, int count,
+                                 void* out_value, double* out_logscale, cudaStream_t stream) {
+  if (precision == RGS_PREC_C128)
+    scan_finalize_kernel<double><<<(count + 127) / 128, 128, 0, stream>>>((const double*)E, maxbuf, n, Bt, count,
+                                                                          (double*)out_value, out_logscale);
+  else
+    scan_finalize_kernel<float><<<(count + 127) / 128, 128, 0, stream>>>((const float*)E, maxbuf, n, Bt, count,
+                                                                         (float*)out_value, out_logscale);
+  return cudaGetLastError();
+}
+
 }  // namespace rgs

@@ -36,4 +36,16 @@ int scan_run(Plan& plan, const double* U, const unsigned long long* bits, const 
              int precision, void* out_value, double* out_logscale, void* workspace, size_t ws_bytes, int Bt,
              cudaStream_t stream, ScanStats* stats);
 
+// Single-kernel launch wrappers (same kernels as scan_run), for drivers that manage
+// their own device memory layout.
+cudaError_t scan_launch_weights(const DevVert* verts, int n, const double* U, const unsigned long long* bits,
+                                const double* fvec, long long first, int count, int Bt, void* W, unsigned char* F,
+                                cudaStream_t stream);
+cudaError_t scan_launch_step(int precision, int Bt, int device, const DevStep& st, const void* Ein, void* Eout,
+                             const unsigned long long* T, const void* W, const unsigned char* F,
+                             const unsigned long long* maxprev, unsigned long long* maxcur, bool unit_input,
+                             cudaStream_t stream);
+cudaError_t scan_launch_finalize(int precision, const void* E, const unsigned long long* maxbuf, int n, int Bt,
+                                 int count, void* out_value, double* out_logscale, cudaStream_t stream);
+
 }  // namespace rgs
