@@ -315,7 +315,7 @@ def run_ours(args, rank, world, local_rank):
                        "instance": inst.name, "rmax": inst.rmax, "sum_states": inst.sum_states,
                        "batch_per_gpu": BATCH, "batch_tile": {"c64": tile64, "c128": tile128},
                        "precisions": args.only,
-                       "l2": "inputs larger than L2 (c64 tables 2 x 4 GiB, c128 2 x 4 GiB)",
+                       "l2": "inputs larger than L2 (tables of 2^20 rows x batch tile, >= 2 x 1 GiB)",
                        "parallelism": f"replicas x{world}"},
             "split": {"c64_amplitudes_per_s": world * BATCH * args.steps / t64 if t64 else None,
                       "c128_amplitudes_per_s": world * BATCH * args.steps / t128 if t128 else None},
@@ -350,8 +350,8 @@ def main():
     ap.add_argument("--only", choices=["both", "c64", "c128"], default="both",
                     help="run only one precision (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
-    ap.add_argument("--tile64", type=int, default=512)
-    ap.add_argument("--tile128", type=int, default=256)
+    ap.add_argument("--tile64", type=int, default=128)
+    ap.add_argument("--tile128", type=int, default=64)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus if args.gpus == 1 else 1))

@@ -88,8 +88,12 @@ int rgs_rank_profile(int32_t n, int32_t n_edges, const int32_t* edges, const int
  *
  * Workspace: caller-owned device memory of at least
  * rgs_scan_workspace_bytes(plan, batch_tile, precision) bytes; batch_tile is a
- * power of two (1..512) = bitstrings executed together in one interleaved table. */
+ * power of two (1..rgs_scan_max_batch_tile) = bitstrings executed together in one
+ * interleaved table. */
 int rgs_scan_workspace_bytes(const rgs_plan* plan, int32_t batch_tile, int32_t precision, size_t* bytes);
+/* Largest batch_tile accepted for a precision (128 complex64, 256 complex64/float32 math,
+ * 64 complex128). */
+int rgs_scan_max_batch_tile(int32_t precision, int32_t* tile);
 
 /* Bitstring interface: f_q = U_q[x_q, :] (W/scan_oracle.py:26).
  * unitaries: device complex128[n][2][2]; bits: device uint64[batch][2];

@@ -145,6 +145,13 @@ int rgs_rank_profile(int32_t n, int32_t n_edges, const int32_t* edges, const int
   return RGS_OK;
 }
 
+int rgs_scan_max_batch_tile(int32_t precision, int32_t* tile) {
+  if (!tile) return fail(RGS_ERR_ARG, "tile is NULL");
+  if (precision < RGS_PREC_C64 || precision > RGS_PREC_C128) return fail(RGS_ERR_ARG, "unknown precision");
+  *tile = scan_max_tile(precision);
+  return RGS_OK;
+}
+
 int rgs_scan_workspace_bytes(const rgs_plan* plan, int32_t batch_tile, int32_t precision, size_t* bytes) {
   if (!plan || !bytes) return fail(RGS_ERR_ARG, "null argument");
   ScanLayout L;

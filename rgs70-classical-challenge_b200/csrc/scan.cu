@@ -19,6 +19,7 @@
 #include "plan.hpp"
 #include "scan.hpp"
 #include "scan_device.cuh"
+#include "scan_row.cuh"
 
 namespace rgs {
 
@@ -148,87 +149,6 @@ __global__ void scan_weights_kernel(const DevVert* __restrict__ verts, int n, co
 }
 
 // ------------------------------------------------------------------------------------------------
-// One scan position over a batch tile.  Grid-stride over items; a thread keeps its V
-// items (lane) for the whole launch, so weights and scales are set up once.
-template <typename S, typename M, int V, int MODE>
-__global__ void __launch_bounds__(256) scan_step_kernel(const S* __restrict__ Ein, S* __restrict__ Eout,
-                                                        const __grid_constant__ DevStep st,
-                                                        const u64* __restrict__ T, const double4* __restrict__ W,
-                                                        const unsigned char* __restrict__ F,
-                                                        const u64* __restrict__ maxprev,
-                                                        u64* __restrict__ maxcur, int lbt, int unit_input) {
-  __shared__ u64 smax[512];
-  const int Bt = 1 << lbt;
-  const int llpr = lbt - (V == 2 ? 1 : 0);  // log2 lanes per row
-  const u64 tid = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = (int)(tid & ((1ull << llpr) - 1ull));
-  const int b0 = lane * V;
-
-  for (int i = threadIdx.x; i < Bt; i += blockDim.x) smax[i] = 0;
-
-  StepWeights<M, V> w;
-#pragma unroll
-  for (int v = 0; v < V; ++v) {
-    const int b = b0 + v;
-    const double m2 = maxprev ? max_value<S>(maxprev[b]) : 1.0;
-    const double s = ldexp(1.0, -scale_exponent(m2));
-    const double4 f = W[b];
-    w.w0[v].re = (M)(f.x * s);
-    w.w0[v].im = (M)(f.y * s);
-    w.w1[v].re = (M)(f.z * s);
-    w.w1[v].im = (M)(f.w * s);
-    const int fl = F ? F[b] : 0;
-    w.y[v] = fl & 1;
-    w.ov[v] = (fl >> 1) & 1;
-  }
-  __syncthreads();
-
-  const u64 items = (MODE == MODE_PAIR) ? (1ull << (st.r_out - 1)) : (1ull << st.r_out);
-  const u64 stride = ((u64)gridDim.x * blockDim.x) >> llpr;
-  S mx[V];
-#pragma unroll
-  for (int v = 0; v < V; ++v) mx[v] = (S)0;
-
-  for (u64 item = tid >> llpr; item < items; item += stride) {
-    u64 ca, cb;
-    Cx<M> oa[V], ob[V];
-    step_item<S, M, V, MODE, RowIO<S, V>>(Ein, st, T, w, item, lbt, b0, unit_input != 0, ca, cb, oa, ob);
-    S ra[V], ia[V];
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      ra[v] = (S)oa[v].re;
-      ia[v] = (S)oa[v].im;
-      mx[v] = fmax(mx[v], ra[v] * ra[v] + ia[v] * ia[v]);
-    }
-    RowIO<S, V>::store(Eout, (ca << lbt) + (u64)b0, ra, ia);
-    if (MODE == MODE_PAIR) {
-#pragma unroll
-      for (int v = 0; v < V; ++v) {
-        ra[v] = (S)ob[v].re;
-        ia[v] = (S)ob[v].im;
-        mx[v] = fmax(mx[v], ra[v] * ra[v] + ia[v] * ia[v]);
-      }
-      RowIO<S, V>::store(Eout, (cb << lbt) + (u64)b0, ra, ia);
-    }
-  }
-
-  // Maximum |E|^2 per item: lanes of one warp that share items first, then shared
-  // memory, then one global atomic per item per block (gpu_kernel.py:98-101).
-#pragma unroll
-  for (int v = 0; v < V; ++v) {
-    u64 bitsv = max_bits<S>(mx[v]);
-    for (int off = 16; off >= (1 << llpr) && off >= 1; off >>= 1) {
-      const u64 o = __shfl_xor_sync(0xffffffffu, bitsv, off);
-      bitsv = bitsv > o ? bitsv : o;
-    }
-    if ((threadIdx.x & 31) < (1 << llpr) && bitsv) atomicMax(&smax[b0 + v], bitsv);
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < Bt; i += blockDim.x)
-    if (smax[i]) atomicMax(&maxcur[i], smax[i]);
-}
-
-// ------------------------------------------------------------------------------------------------
 // Final value and log-scale per item (gpu_kernel.py:126-170): value = E[0], logscale =
 // ln2 * sum_j e_j, with e_0 = 1 and e_j from the maximum after step j-1.  An all-zero
 // table ends the sum as in the reference (value 0); a non-finite maximum yields NaN.
@@ -262,6 +182,13 @@ __global__ void scan_finalize_kernel(const S* __restrict__ E, const u64* __restr
 }
 
 // ------------------------------------------------------------------------------------------------
+// Largest batch tile per precision: a lane owns at most 2 chunks (4 for float32 math).
+int scan_max_tile(int precision) {
+  if (precision == RGS_PREC_C128) return 64;
+  if (precision == RGS_PREC_C64_F32) return 256;
+  return 128;
+}
+
 size_t ScanLayout::total() const { return off_max + bytes_max; }
 
 int scan_layout(const Plan& plan, int Bt, int precision, ScanLayout& L) {
@@ -269,8 +196,8 @@ int scan_layout(const Plan& plan, int Bt, int precision, ScanLayout& L) {
   if (precision < RGS_PREC_C64 || precision > RGS_PREC_C128) return fail(RGS_ERR_ARG, "unknown precision");
   if (!plan.exec_ok) return fail(RGS_ERR_UNSUPPORTED, plan.exec_reason);
   const size_t esize = precision == RGS_PREC_C128 ? 16 : 8;
-  // A row of Bt items must be covered by at most one 256-thread block (16 bytes per thread).
-  if ((size_t)Bt * esize > 256 * 16) return fail(RGS_ERR_ARG, "batch_tile too large for complex128 (max 256)");
+  if (Bt > scan_max_tile(precision))
+    return fail(RGS_ERR_ARG, "batch_tile above the maximum for this precision (rgs_scan_max_batch_tile)");
   L.Bt = Bt;
   L.esize = esize;
   L.bytes_buf = align_up(((size_t)1 << plan.rmax) * (size_t)Bt * esize, 256);
@@ -287,36 +214,75 @@ int scan_layout(const Plan& plan, int Bt, int precision, ScanLayout& L) {
 
 namespace {
 
-template <typename S, typename M, int V>
-cudaError_t launch_step_v(int mode, dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevStep& st,
-                          const u64* T, const double4* W, const unsigned char* F, const u64* mp, u64* mc, int lbt,
-                          int unit) {
-  const S* in = (const S*)Ein;
-  S* out = (S*)Eout;
-  switch (mode) {
-    case MODE_PAIR:
-      scan_step_kernel<S, M, V, MODE_PAIR><<<grid, 256, 0, s>>>(in, out, st, T, W, F, mp, mc, lbt, unit);
-      break;
-    case MODE_MERGE:
-      scan_step_kernel<S, M, V, MODE_MERGE><<<grid, 256, 0, s>>>(in, out, st, T, W, F, mp, mc, lbt, unit);
-      break;
-    default:
-      scan_step_kernel<S, M, V, MODE_FIXED><<<grid, 256, 0, s>>>(in, out, st, T, W, F, mp, mc, lbt, unit);
-      break;
-  }
+template <typename S, typename M, int VE, int CPL, int MODE, int NC>
+cudaError_t launch_row(dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevStep& st, const u64* T,
+                       const double4* W, const unsigned char* F, const u64* mp, u64* mc, int lbt, int unit) {
+  scan_row_kernel<S, M, VE, MODE, NC, CPL><<<grid, 256, 0, s>>>((const S*)Ein, (S*)Eout, st, T, W, F, mp, mc, lbt,
+                                                                unit);
   return cudaGetLastError();
 }
 
-cudaError_t launch_step(int precision, int V, int mode, dim3 grid, cudaStream_t s, const void* Ein, void* Eout,
-                        const DevStep& st, const u64* T, const double4* W, const unsigned char* F, const u64* mp,
-                        u64* mc, int lbt, int unit) {
-  if (precision == RGS_PREC_C128) return launch_step_v<double, double, 1>(mode, grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
-  if (precision == RGS_PREC_C64) {
-    if (V == 2) return launch_step_v<float, double, 2>(mode, grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
-    return launch_step_v<float, double, 1>(mode, grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+template <typename S, typename M, int VE, int CPL>
+cudaError_t launch_modes(dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevStep& st, const u64* T,
+                         const double4* W, const unsigned char* F, const u64* mp, u64* mc, int lbt, int unit) {
+#define RGS_ROW(MODE, NC) launch_row<S, M, VE, CPL, MODE, NC>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit)
+  if (st.mode == MODE_PAIR) {
+    if (st.ncombos == 1) return RGS_ROW(MODE_PAIR, 1);
+    if (st.ncombos == 2) return RGS_ROW(MODE_PAIR, 2);
+    return RGS_ROW(MODE_PAIR, 4);
   }
-  if (V == 2) return launch_step_v<float, float, 2>(mode, grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
-  return launch_step_v<float, float, 1>(mode, grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+  if (st.mode == MODE_MERGE) {
+    if (st.ncombos == 1) return RGS_ROW(MODE_MERGE, 1);
+    return RGS_ROW(MODE_MERGE, 2);
+  }
+  if (st.ncombos == 1) return RGS_ROW(MODE_FIXED, 1);
+  return RGS_ROW(MODE_FIXED, 2);
+#undef RGS_ROW
+}
+
+// Launch geometry of one step: chunk size, chunks per lane, and a grid of 256-thread
+// blocks with enough warps for every row (capped; the kernel strides over the rest).
+struct StepGeometry {
+  int VE, CPL;
+  long long blocks;
+};
+
+StepGeometry step_geometry(int precision, int Bt, const DevStep& st, int device) {
+  StepGeometry g;
+  const int lbt = __builtin_ctz((unsigned)Bt);
+  g.VE = (precision != RGS_PREC_C128 && Bt >= 2) ? 2 : 1;
+  const int lC = lbt - (g.VE == 2 ? 1 : 0);
+  const int lL = lC < 5 ? lC : 5;
+  g.CPL = 1 << (lC - lL);
+  const int loads = precision == RGS_PREC_C64 ? 4 : 8;  // LoadsInFlight of the kernel
+  const int U = (st.ncombos * g.CPL >= loads) ? 1 : loads / (st.ncombos * g.CPL);
+  const unsigned long long items = st.mode == MODE_PAIR ? (1ull << (st.r_out - 1)) : (1ull << st.r_out);
+  const unsigned long long per_warp = (unsigned long long)U << (5 - lL);
+  const unsigned long long warps = (items + per_warp - 1) / per_warp;
+  const long long cap = (long long)sm_count(device) * 16;
+  g.blocks = std::max<long long>(1, std::min<long long>((long long)((warps + 7) / 8), cap));
+  return g;
+}
+
+cudaError_t launch_step(int precision, int Bt, int device, cudaStream_t s, const void* Ein, void* Eout,
+                        const DevStep& st, const u64* T, const double4* W, const unsigned char* F, const u64* mp,
+                        u64* mc, int unit) {
+  const StepGeometry g = step_geometry(precision, Bt, st, device);
+  const int lbt = __builtin_ctz((unsigned)Bt);
+  const dim3 grid((unsigned)g.blocks);
+  if (precision == RGS_PREC_C128) {
+    if (g.CPL == 1) return launch_modes<double, double, 1, 1>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+    return launch_modes<double, double, 1, 2>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+  }
+  if (precision == RGS_PREC_C64) {
+    if (g.VE == 1) return launch_modes<float, double, 1, 1>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+    if (g.CPL == 1) return launch_modes<float, double, 2, 1>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+    return launch_modes<float, double, 2, 2>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+  }
+  if (g.VE == 1) return launch_modes<float, float, 1, 1>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+  if (g.CPL == 1) return launch_modes<float, float, 2, 1>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+  if (g.CPL == 2) return launch_modes<float, float, 2, 2>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+  return launch_modes<float, float, 2, 4>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
 }
 
 bool plan_has_fixed(const Plan& p) {
@@ -352,12 +318,6 @@ int scan_run(Plan& plan, const double* U, const u64* bits, const double* fvec, l
   unsigned char* F = plan_has_fixed(plan) ? (unsigned char*)(ws + L.off_f) : nullptr;
   u64* maxbuf = (u64*)(ws + L.off_max);
   const u64* tables = (const u64*)dc->tables;
-  const int lbt = __builtin_ctz((unsigned)Bt);
-  const int V = (precision != RGS_PREC_C128 && Bt >= 2) ? 2 : 1;
-  const int lpr = Bt / V;
-  const int sms = sm_count(device);
-  const long long max_blocks = (long long)sms * 8;
-  const size_t esize = L.esize;
   long long launches = 0;
 
   for (long long first = 0; first < batch; first += Bt) {
@@ -369,12 +329,9 @@ int scan_run(Plan& plan, const double* U, const u64* bits, const double* fvec, l
     launches += 1;
     for (int j = 0; j < plan.n; ++j) {
       const DevStep& st = plan.dev[j];
-      const u64 items = st.mode == MODE_PAIR ? (1ull << (st.r_out - 1)) : (1ull << st.r_out);
-      const long long threads = (long long)items * lpr;
-      const long long blocks = std::max<long long>(1, std::min<long long>((threads + 255) / 256, max_blocks));
-      RGS_CUDA_TRY(launch_step(precision, V, st.mode, dim3((unsigned)blocks), stream, buf[j & 1], buf[(j + 1) & 1], st,
-                               tables + st.table_off, W + (size_t)j * Bt, F ? F + (size_t)j * Bt : nullptr,
-                               j ? maxbuf + (size_t)(j - 1) * Bt : nullptr, maxbuf + (size_t)j * Bt, lbt, j == 0));
+      RGS_CUDA_TRY(launch_step(precision, Bt, device, stream, buf[j & 1], buf[(j + 1) & 1], st, tables + st.table_off,
+                               W + (size_t)j * Bt, F ? F + (size_t)j * Bt : nullptr,
+                               j ? maxbuf + (size_t)(j - 1) * Bt : nullptr, maxbuf + (size_t)j * Bt, j == 0));
       launches += 1;
     }
     const void* fin = buf[plan.n & 1];
@@ -387,7 +344,6 @@ int scan_run(Plan& plan, const double* U, const u64* bits, const double* fvec, l
     RGS_CUDA_TRY(cudaGetLastError());
     launches += 1;
   }
-  (void)esize;
   if (stats) stats->launches = launches;
   return RGS_OK;
 }
@@ -403,14 +359,8 @@ cudaError_t scan_launch_weights(const DevVert* verts, int n, const double* U, co
 cudaError_t scan_launch_step(int precision, int Bt, int device, const DevStep& st, const void* Ein, void* Eout,
                              const u64* T, const void* W, const unsigned char* F, const u64* maxprev, u64* maxcur,
                              bool unit_input, cudaStream_t stream) {
-  const int lbt = __builtin_ctz((unsigned)Bt);
-  const int V = (precision != RGS_PREC_C128 && Bt >= 2) ? 2 : 1;
-  const u64 items = st.mode == MODE_PAIR ? (1ull << (st.r_out - 1)) : (1ull << st.r_out);
-  const long long threads = (long long)items * (Bt / V);
-  const long long max_blocks = (long long)sm_count(device) * 8;
-  const long long blocks = std::max<long long>(1, std::min<long long>((threads + 255) / 256, max_blocks));
-  return launch_step(precision, V, st.mode, dim3((unsigned)blocks), stream, Ein, Eout, st, T, (const double4*)W, F,
-                     maxprev, maxcur, lbt, unit_input ? 1 : 0);
+  return launch_step(precision, Bt, device, stream, Ein, Eout, st, T, (const double4*)W, F, maxprev, maxcur,
+                     unit_input ? 1 : 0);
 }
 
 cudaError_t scan_launch_finalize(int precision, const void* E, const u64* maxbuf, int n, int Bt, int count,

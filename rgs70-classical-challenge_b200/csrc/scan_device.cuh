@@ -3,9 +3,9 @@
 // resident sweep and the chain-rule sampler.
 //
 // Table layout: complex entries interleaved over a batch tile of Bt = 2^lbt
-// items, E[c][b] (b fastest).  A thread owns V consecutive items of one row, so a
-// gather of row c is one 8- or 16-byte load per thread and lpr = Bt/V threads
-// cover the row: 128-bit coalesced for complex64 with Bt >= 2.
+// items, E[c][b] (b fastest).  A row is cut into 16-byte chunks (two complex64 or
+// one complex128 values); lanes of a warp own consecutive chunks, so a gather of
+// row c is a fully coalesced run of 128-bit loads.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -26,83 +26,53 @@ __device__ __forceinline__ void cmad(Cx<M>& acc, M er, M ei, const Cx<M>& w) {
   acc.im += er * w.im + ei * w.re;
 }
 
-// Loads V complex values of row `row` at item offset b0.  S = storage real type.
-template <typename S, int V>
-struct RowIO;
-
+// One 16-byte (or, for single-item complex64 rows, 8-byte) chunk of a table row:
+// VE consecutive complex values of storage type S.
+template <typename S, int VE>
+struct Chunk;
 template <>
-struct RowIO<float, 1> {
-  static __device__ __forceinline__ void load(const float* E, u64 idx, float (&re)[1], float (&im)[1]) {
-    float2 x = __ldg(reinterpret_cast<const float2*>(E) + idx);
-    re[0] = x.x;
-    im[0] = x.y;
+struct Chunk<float, 2> {
+  float4 v;
+  __device__ __forceinline__ void load(const float* E, u64 chunk) {
+    v = __ldg(reinterpret_cast<const float4*>(E) + chunk);
   }
-  static __device__ __forceinline__ void store(float* E, u64 idx, const float (&re)[1], const float (&im)[1]) {
-    reinterpret_cast<float2*>(E)[idx] = make_float2(re[0], im[0]);
+  __device__ __forceinline__ void store(float* E, u64 chunk) const { reinterpret_cast<float4*>(E)[chunk] = v; }
+  __device__ __forceinline__ float re(int i) const { return i ? v.z : v.x; }
+  __device__ __forceinline__ float im(int i) const { return i ? v.w : v.y; }
+  __device__ __forceinline__ void set(int i, float r, float m) {
+    if (i) {
+      v.z = r;
+      v.w = m;
+    } else {
+      v.x = r;
+      v.y = m;
+    }
   }
+  __device__ __forceinline__ void unit() { v = make_float4(1.f, 0.f, 1.f, 0.f); }
 };
 template <>
-struct RowIO<float, 2> {
-  static __device__ __forceinline__ void load(const float* E, u64 idx, float (&re)[2], float (&im)[2]) {
-    float4 x = __ldg(reinterpret_cast<const float4*>(reinterpret_cast<const float2*>(E) + idx));
-    re[0] = x.x;
-    im[0] = x.y;
-    re[1] = x.z;
-    im[1] = x.w;
+struct Chunk<float, 1> {
+  float2 v;
+  __device__ __forceinline__ void load(const float* E, u64 chunk) {
+    v = __ldg(reinterpret_cast<const float2*>(E) + chunk);
   }
-  static __device__ __forceinline__ void store(float* E, u64 idx, const float (&re)[2], const float (&im)[2]) {
-    *reinterpret_cast<float4*>(reinterpret_cast<float2*>(E) + idx) = make_float4(re[0], im[0], re[1], im[1]);
-  }
+  __device__ __forceinline__ void store(float* E, u64 chunk) const { reinterpret_cast<float2*>(E)[chunk] = v; }
+  __device__ __forceinline__ float re(int) const { return v.x; }
+  __device__ __forceinline__ float im(int) const { return v.y; }
+  __device__ __forceinline__ void set(int, float r, float m) { v = make_float2(r, m); }
+  __device__ __forceinline__ void unit() { v = make_float2(1.f, 0.f); }
 };
 template <>
-struct RowIO<double, 1> {
-  static __device__ __forceinline__ void load(const double* E, u64 idx, double (&re)[1], double (&im)[1]) {
-    double2 x = __ldg(reinterpret_cast<const double2*>(E) + idx);
-    re[0] = x.x;
-    im[0] = x.y;
+struct Chunk<double, 1> {
+  double2 v;
+  __device__ __forceinline__ void load(const double* E, u64 chunk) {
+    v = __ldg(reinterpret_cast<const double2*>(E) + chunk);
   }
-  static __device__ __forceinline__ void store(double* E, u64 idx, const double (&re)[1], const double (&im)[1]) {
-    reinterpret_cast<double2*>(E)[idx] = make_double2(re[0], im[0]);
-  }
-};
-
-// Generic-address variants (shared or global) without the read-only cache hint.
-template <typename S, int V>
-struct RowIOGeneric;
-template <>
-struct RowIOGeneric<float, 1> {
-  static __device__ __forceinline__ void load(const float* E, u64 idx, float (&re)[1], float (&im)[1]) {
-    float2 x = reinterpret_cast<const float2*>(E)[idx];
-    re[0] = x.x;
-    im[0] = x.y;
-  }
-  static __device__ __forceinline__ void store(float* E, u64 idx, const float (&re)[1], const float (&im)[1]) {
-    reinterpret_cast<float2*>(E)[idx] = make_float2(re[0], im[0]);
-  }
-};
-template <>
-struct RowIOGeneric<float, 2> {
-  static __device__ __forceinline__ void load(const float* E, u64 idx, float (&re)[2], float (&im)[2]) {
-    float4 x = *reinterpret_cast<const float4*>(reinterpret_cast<const float2*>(E) + idx);
-    re[0] = x.x;
-    im[0] = x.y;
-    re[1] = x.z;
-    im[1] = x.w;
-  }
-  static __device__ __forceinline__ void store(float* E, u64 idx, const float (&re)[2], const float (&im)[2]) {
-    *reinterpret_cast<float4*>(reinterpret_cast<float2*>(E) + idx) = make_float4(re[0], im[0], re[1], im[1]);
-  }
-};
-template <>
-struct RowIOGeneric<double, 1> {
-  static __device__ __forceinline__ void load(const double* E, u64 idx, double (&re)[1], double (&im)[1]) {
-    double2 x = reinterpret_cast<const double2*>(E)[idx];
-    re[0] = x.x;
-    im[0] = x.y;
-  }
-  static __device__ __forceinline__ void store(double* E, u64 idx, const double (&re)[1], const double (&im)[1]) {
-    reinterpret_cast<double2*>(E)[idx] = make_double2(re[0], im[0]);
-  }
+  __device__ __forceinline__ void store(double* E, u64 chunk) const { reinterpret_cast<double2*>(E)[chunk] = v; }
+  __device__ __forceinline__ double re(int) const { return v.x; }
+  __device__ __forceinline__ double im(int) const { return v.y; }
+  __device__ __forceinline__ void set(int, double r, double m) { v = make_double2(r, m); }
+  __device__ __forceinline__ void unit() { v = make_double2(1.0, 0.0); }
 };
 
 // p0 = L c' by XOR of byte tables (scan_plan.py:133-145, gpu_kernel.py:73-75).
@@ -148,99 +118,6 @@ __device__ __forceinline__ double max_value<float>(u64 bits) {
 template <>
 __device__ __forceinline__ double max_value<double>(u64 bits) {
   return __longlong_as_double((long long)bits);
-}
-
-// Per-thread weights of one scan position for its V items: f(0), f(1) scaled by
-// 2^-e, plus the fixed-vertex value y and the syndrome-offset bit ov.
-template <typename M, int V>
-struct StepWeights {
-  Cx<M> w0[V], w1[V];
-  int y[V], ov[V];
-};
-
-// One output pair / output of a step (see StepMode).  Returns the values; the
-// caller stores them.  E is addressed through IO (global or shared).
-template <typename S, typename M, int V, int MODE, class IO>
-__device__ __forceinline__ void step_item(const S* __restrict__ E, const DevStep& st, const u64* __restrict__ T,
-                                          const StepWeights<M, V>& w, u64 item, int lbt, int b0, bool unit_input,
-                                          u64& ca, u64& cb, Cx<M> (&oa)[V], Cx<M> (&ob)[V]) {
-  const u64 mask = (1ull << st.r_in) - 1ull;
-#pragma unroll
-  for (int v = 0; v < V; ++v) {
-    oa[v].re = oa[v].im = ob[v].re = ob[v].im = (M)0;
-  }
-  if (MODE == MODE_PAIR) {
-    ca = deposit_zero(item, st.pi);
-    cb = ca ^ st.t;
-  } else {
-    ca = item;
-    cb = item;
-  }
-  const u64 p0 = table_lookup(T, st.nbytes, ca);
-  // Issue every gather first (at most four rows), then the arithmetic.
-  S er[4][V], ei[4][V];
-  u64 pk[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    pk[k] = p0 ^ st.combos[k];
-    if (k < st.ncombos) {
-      const u64 c = pk[k] & mask;
-      if (unit_input) {
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-          er[k][v] = (S)1;
-          ei[k][v] = (S)0;
-        }
-      } else {
-        IO::load(E, (c << lbt) + (u64)b0, er[k], ei[k]);
-      }
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (k >= st.ncombos) break;
-    const u64 c = pk[k] & mask;
-    const int pc = __popcll(c & st.beta) & 1;
-    if (MODE == MODE_PAIR) {
-      const int y = (int)((pk[k] >> st.r_in) & 1ull);
-#pragma unroll
-      for (int v = 0; v < V; ++v) {
-        const int par = pc ^ w.ov[v];
-        Cx<M> wa = y ? w.w1[v] : w.w0[v];
-        Cx<M> wb = y ? w.w0[v] : w.w1[v];
-        if (y & par) {
-          wa.re = -wa.re;
-          wa.im = -wa.im;
-        }
-        if ((y ^ 1) & par) {
-          wb.re = -wb.re;
-          wb.im = -wb.im;
-        }
-        cmad(oa[v], (M)er[k][v], (M)ei[k][v], wa);
-        cmad(ob[v], (M)er[k][v], (M)ei[k][v], wb);
-      }
-    } else if (MODE == MODE_MERGE) {
-#pragma unroll
-      for (int v = 0; v < V; ++v) {
-        const int par = pc ^ w.ov[v];
-        Cx<M> ww;
-        ww.re = par ? w.w0[v].re - w.w1[v].re : w.w0[v].re + w.w1[v].re;
-        ww.im = par ? w.w0[v].im - w.w1[v].im : w.w0[v].im + w.w1[v].im;
-        cmad(oa[v], (M)er[k][v], (M)ei[k][v], ww);
-      }
-    } else {  // MODE_FIXED
-#pragma unroll
-      for (int v = 0; v < V; ++v) {
-        const int par = pc ^ w.ov[v];
-        Cx<M> ww = w.y[v] ? w.w1[v] : w.w0[v];
-        if (w.y[v] & par) {
-          ww.re = -ww.re;
-          ww.im = -ww.im;
-        }
-        cmad(oa[v], (M)er[k][v], (M)ei[k][v], ww);
-      }
-    }
-  }
 }
 
 }  // namespace rgs

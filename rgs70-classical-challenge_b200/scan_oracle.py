@@ -19,7 +19,7 @@ import torch
 from . import _lib
 from .plan import ScanPlan, edges_from_graph
 
-__all__ = ["ScanEngine", "ScanOracle", "pack_bits", "PRECISIONS"]
+__all__ = ["ScanEngine", "ScanOracle", "pack_bits", "PRECISIONS", "max_batch_tile"]
 
 PRECISIONS = {"c64": _lib.PREC_C64, "c64f32": _lib.PREC_C64_F32, "c128": _lib.PREC_C128}
 LN2 = math.log(2.0)
@@ -41,9 +41,16 @@ def pack_bits(bits, n=None):
     return np.ascontiguousarray(np.packbits(padded, axis=1, bitorder="little").view("<u8"))
 
 
-def _auto_tile(batch, rmax, esize, budget):
+def max_batch_tile(precision):
+    """Largest batch tile the step kernel accepts for a precision name."""
+    t = ctypes.c_int32()
+    _lib.check(_lib.lib().rgs_scan_max_batch_tile(PRECISIONS[precision], ctypes.byref(t)))
+    return int(t.value)
+
+
+def _auto_tile(batch, rmax, esize, budget, cap):
+    """Largest power-of-two tile <= cap and <= batch whose two tables fit the budget."""
     bt = 1
-    cap = 512 if esize == 8 else 256
     while bt * 2 <= min(cap, max(1, batch)) and 2 * (bt * 2) * esize * (1 << rmax) <= budget:
         bt *= 2
     while bt > 1 and 2 * bt * esize * (1 << rmax) > budget:
@@ -83,7 +90,7 @@ class ScanEngine:
     def tile_for(self, batch):
         if self.batch_tile is not None:
             return int(self.batch_tile)
-        return _auto_tile(batch, self.plan.rmax, self.esize, self.memory_budget)
+        return _auto_tile(batch, self.plan.rmax, self.esize, self.memory_budget, max_batch_tile(self.precision))
 
     def workspace_bytes(self, tile):
         nb = ctypes.c_size_t()
