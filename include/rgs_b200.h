@@ -109,6 +109,61 @@ int rgs_scan_contract(rgs_plan* plan, const double* fvec, int64_t batch, int32_t
                       void* out_value, double* out_logscale, void* workspace, size_t workspace_bytes,
                       int32_t batch_tile, void* stream);
 
+/* ---------------------------------------------------------------- conditional (Fourier-cut) sampler
+ * Replaces DistributedSampler / FourierCovariantSampler / FusedFourierSampler /
+ * DeferredGlobalMixin / SpecializedDeferredSampler (W/distributed_sampler.py:59-162,
+ * W/fourier_covariant_sampler.py:97-141, W/fourier_fused_sampler.py:288-336,
+ * W/deferred_global_sampler.py:40-88, W/specialized_deferred_sampler.py:204-238,
+ * W/init_specialization.py:160-246) on one device.  Requires a balanced cut with
+ * rank(G[B,A]) = |B| = m (RGS_ERR_SINGULAR otherwise), 4 <= m <= 40.
+ * graph: host uint8[n][n]; unitaries: host complex128[n][2][2]; A, B: host int32[m].
+ * deferred != 0 applies the unitary of A[m-1] at draw time (deferred_global_sampler.py:1-8).
+ * The state is caller-owned device complex64[2^m]; outB bit j = outcome of B[j]. */
+typedef struct rgs_fourier rgs_fourier;
+int rgs_fourier_create(int32_t n, const uint8_t* graph, const double* unitaries, int32_t m, const int32_t* A,
+                       const int32_t* B, int32_t deferred, rgs_fourier** out);
+void rgs_fourier_destroy(rgs_fourier* plan);
+/* m, whether the identical-B lookup specialisation is used, tile bits, tiles, passes. */
+int rgs_fourier_info(const rgs_fourier* plan, int32_t* m, int32_t* specialized, int32_t* tile_bits,
+                     int64_t* ntiles, int32_t* passes);
+/* GF(2) tables for parity tests (init_specialization.py:176-188 layout):
+ * lut_z uint64[chunks][256][2] (b XOR, phase mask | inner << 63) of the covariant map,
+ * lut_a uint64[chunks][256][2] of q_A, lut_cols uint64[chunks][256][2] of the index map,
+ * inv_rows uint64[m] rows of N = G[B,A]^{-T}.  Any pointer may be NULL. */
+int rgs_fourier_tables(const rgs_fourier* plan, uint64_t* lut_z, uint64_t* lut_a, uint64_t* lut_cols,
+                       uint64_t* inv_rows, int32_t* chunks);
+int rgs_fourier_workspace_bytes(const rgs_fourier* plan, size_t* bytes);
+/* Conditional state for outB (compute(outB), specialized_deferred_sampler.py:222-238):
+ * init + WHT + q_A phase + products, tile masses into the workspace.  stage_ms: NULL, or
+ * float[3] for device times of (init, walsh, product) -- then the call synchronises. */
+int rgs_fourier_compute(rgs_fourier* plan, uint64_t outB, void* state, void* workspace, size_t workspace_bytes,
+                        void* stream, float* stage_ms);
+/* The reference base pipeline (distributed_sampler.py:126-144): product init over b,
+ * WHT, index map with q_A phase into `scratch`, products; result in `scratch`. */
+int rgs_fourier_compute_permute(rgs_fourier* plan, uint64_t outB, void* state, void* scratch, void* workspace,
+                                size_t workspace_bytes, void* stream);
+/* Tile masses (float64) of a state (masses(), distributed_sampler.py:145-152); synchronises. */
+int rgs_fourier_masses(rgs_fourier* plan, const void* state, void* workspace, double* host_masses, double* norm,
+                       void* stream);
+/* Two-level inverse CDF over tile masses with uniforms u1, u2, then the deferred
+ * terminal pair with u3 (draw(), deferred_global_sampler.py:72-78); synchronises.
+ * Fails with RGS_ERR_ZERO_NORM when |norm - 1| > 1e-3 (distributed_sampler.py:151). */
+int rgs_fourier_draw(rgs_fourier* plan, const void* state, void* workspace, double u1, double u2, double u3,
+                     uint64_t* index, double* pa, double* norm, void* stream);
+/* Index map with q_A phase (permute, distributed_sampler.py:35-41), dst != src. */
+int rgs_fourier_index_map(rgs_fourier* plan, const void* src, void* dst, void* stream);
+/* state[z] *= (-1)^{q_A(z)} (quadratic_phase, graph_sampler.py:76-85). */
+int rgs_fourier_quadphase(rgs_fourier* plan, void* state, void* stream);
+
+/* Building blocks on a device complex64 state of 2^nbits values (nbits >= 4), in place. */
+/* Walsh-Hadamard butterflies on bits [lo, hi) (lowfwht/localfwht/fusedfwht). */
+int rgs_fwht(void* state, int32_t nbits, int32_t lo, int32_t hi, void* stream);
+/* Per-qubit 2x2 products on bits [lo, hi); unitaries: device complex128[nbits][2][2]
+ * (lowprod/localprod/fusedprod). */
+int rgs_product(void* state, int32_t nbits, const double* unitaries, int32_t lo, int32_t hi, void* stream);
+/* masses[t] = sum |state|^2 over tile t of 2^tile_bits (blockmass, distributed_sampler.py:50-54). */
+int rgs_block_mass(const void* state, int32_t nbits, int32_t tile_bits, double* masses, void* stream);
+
 /* ---------------------------------------------------------------- allocation-free scan
  * No counterpart in the reference.  Same result as rgs_scan_amplitudes, for callers
  * that cannot allocate device memory at call time (host callbacks, hosts that give

@@ -10,8 +10,10 @@ from .plan import ScanPlan, Step, make_plan, future_masks, rank_profile, byte_ta
     edges_from_graph
 from .scan_oracle import ScanEngine, ScanOracle, pack_bits, amplitudes_from, PRECISIONS
 from . import instances
+from .samplers import ConditionalSampler, DrawRecorder, produce, fwht, product, block_mass
 
 __all__ = [
     "ScanPlan", "Step", "make_plan", "future_masks", "rank_profile", "byte_tables", "kernel_combos",
     "edges_from_graph", "ScanEngine", "ScanOracle", "pack_bits", "amplitudes_from", "PRECISIONS",
+    "ConditionalSampler", "DrawRecorder", "produce", "fwht", "product", "block_mass",
 ]

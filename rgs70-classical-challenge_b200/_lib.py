@@ -67,6 +67,25 @@ SIGNATURES = {
                                          c_void_p, c_void_p, ctypes.c_size_t, ctypes.c_int32, c_void_p]),
     "rgs_scan_amplitudes_noalloc": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_int64, ctypes.c_int32,
                                                    c_void_p, c_void_p, c_void_p]),
+    "rgs_fourier_create": (ctypes.c_int, [ctypes.c_int32, c_uint8_p, c_double_p, ctypes.c_int32, c_int32_p,
+                                          c_int32_p, ctypes.c_int32, ctypes.POINTER(c_void_p)]),
+    "rgs_fourier_destroy": (None, [c_void_p]),
+    "rgs_fourier_info": (ctypes.c_int, [c_void_p, c_int32_p, c_int32_p, c_int32_p, ctypes.POINTER(ctypes.c_int64),
+                                        c_int32_p]),
+    "rgs_fourier_tables": (ctypes.c_int, [c_void_p, c_uint64_p, c_uint64_p, c_uint64_p, c_uint64_p, c_int32_p]),
+    "rgs_fourier_workspace_bytes": (ctypes.c_int, [c_void_p, c_size_t_p]),
+    "rgs_fourier_compute": (ctypes.c_int, [c_void_p, ctypes.c_uint64, c_void_p, c_void_p, ctypes.c_size_t, c_void_p,
+                                           ctypes.POINTER(ctypes.c_float)]),
+    "rgs_fourier_compute_permute": (ctypes.c_int, [c_void_p, ctypes.c_uint64, c_void_p, c_void_p, c_void_p,
+                                                   ctypes.c_size_t, c_void_p]),
+    "rgs_fourier_masses": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_double_p, c_double_p, c_void_p]),
+    "rgs_fourier_draw": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double, c_uint64_p, c_double_p, c_double_p, c_void_p]),
+    "rgs_fourier_index_map": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "rgs_fourier_quadphase": (ctypes.c_int, [c_void_p, c_void_p, c_void_p]),
+    "rgs_fwht": (ctypes.c_int, [c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_void_p]),
+    "rgs_product": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_void_p, ctypes.c_int32, ctypes.c_int32, c_void_p]),
+    "rgs_block_mass": (ctypes.c_int, [c_void_p, ctypes.c_int32, ctypes.c_int32, c_void_p, c_void_p]),
 }
 
 _lib = None

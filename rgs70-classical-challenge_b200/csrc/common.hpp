@@ -32,4 +32,9 @@ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 int sm_count(int device);
 
+// The library carries its own CUDA runtime, whose current device is independent of the
+// caller's runtime: make the device that owns the caller's pointer `p` current and
+// return it.
+int bind_device_of(const void* p, int* device);
+
 }  // namespace rgs

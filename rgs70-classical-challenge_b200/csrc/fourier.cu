@@ -1,0 +1,822 @@
+// Conditional (Fourier-cut) sampler on one B200.
+//
+// Replaces the multi-kernel CuPy pipeline of whyihaveyou/rgs70-classical-challenge
+// (W/ = work/rgs_attack/): initialisation (initv / initcov / initcov_specialized*,
+// W/distributed_sampler.py:14-20, W/fourier_covariant_sampler.py:78-86,
+// W/init_specialization.py:196-246), Walsh-Hadamard transform (lowfwht / localfwht /
+// fusedfwht, distributed_sampler.py:21-31, fourier_fused_sampler.py:19-32), q_A phase and
+// per-qubit products (lowprod / localprod / lowprodphase / fusedprod), the index map
+// (permute, distributed_sampler.py:35-41) and tile masses + draw (blockmass / draw,
+// distributed_sampler.py:50-54, 145-157; deferred_global_sampler.py:65-78).
+//
+// Pass structure.  The state is 2^m complex64 values in HBM.  A pass streams it once
+// in tiles of 2^13 elements staged in shared memory: either a contiguous tile (the 13
+// low bits) or a strided tile (3 contiguous low bits = 64-byte runs, times up to 10
+// "target" bits at position q).  Inside a tile each thread holds 16 elements in
+// registers along 4 tile axes and applies every 2x2 operation on those axes; four-axis
+// rounds are separated by a swizzled shared-memory exchange.  The whole transform is
+//   pass 0          : init (computed, not loaded) + WHT on bits [0, 13)
+//   strided passes  : WHT on the next groups of 10 bits
+//   middle pass     : WHT on the last group, q_A phase, products on that group
+//   strided passes  : products on the earlier groups (reverse order)
+//   last pass       : products on bits [0, 13) + per-tile masses (float64)
+// = 2k+1 passes for m = 13 + 10k bits: 8 + 16*2k bytes per element (the reference
+// streams 2 + 2*ceil((m-10)/5) passes of 16 bytes, plus a mass pass).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+
+#include "common.hpp"
+#include "fourier.cuh"
+
+namespace rgs {
+
+typedef unsigned long long u64;
+
+FourierPlan::~FourierPlan() {
+  if (device < 0) return;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device);
+  for (void* p : {d_lut_z, d_lut_a, d_lut_cols, d_uA, d_uB})
+    if (p) cudaFree(p);
+  if (prev >= 0) cudaSetDevice(prev);
+}
+
+namespace {
+
+// ------------------------------------------------------------------------------------- device
+enum InitKind : int { INIT_LOAD = 0, INIT_COV_GENERIC = 1, INIT_COV_SPECIAL = 2, INIT_PRODUCT = 3 };
+
+struct PassParams {
+  float2* v;
+  int m, c, K, q;                 // tile = c low bits + K target bits at q
+  unsigned wht_mask, u_mask;      // tile-local axes
+  int phase;                      // q_A phase after the WHT rounds
+  int init;                       // InitKind
+  int chunks;
+  const u64* lut_z;               // covariant map + q_B (INIT_COV_*), or q_B over b (INIT_PRODUCT)
+  const u64* lut_a;               // q_A
+  const double2* wgen;            // [chunks][256] complex128 chunk weights
+  const double2* wspec;           // [(m+1)^2] popcount weights
+  u64 outmask;
+  const double2* u;               // [m][2][2] complex128 per global bit
+  double* masses;                 // per tile or null
+  int store;
+};
+
+__device__ __forceinline__ int swz(int f) { return f ^ ((f >> 4) & 15); }
+
+__device__ __forceinline__ u64 tile_global(const PassParams& P, u64 tile, int f) {
+  const int mid = P.q - P.c;  // bits between the low part and the target bits
+  const u64 base = ((tile & ((1ull << mid) - 1ull)) << P.c) | ((tile >> mid) << (P.q + P.K));
+  return base | (u64)(f & ((1 << P.c) - 1)) | ((u64)(f >> P.c) << P.q);
+}
+
+__device__ __forceinline__ int local_to_global_bit(const PassParams& P, int a) {
+  return a < P.c ? a : P.q + (a - P.c);
+}
+
+__device__ __forceinline__ u64 lut_parity_mask(const u64* lut, int chunks, u64 z) {
+  const u64 marked = z | (1ull << 63);
+  u64 pm = 0;
+  for (int cc = 0; cc < chunks; ++cc) pm ^= __ldg(lut + ((((u64)cc << 8) + ((z >> (8 * cc)) & 255ull)) << 1) + 1) & marked;
+  return pm;
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// Initial value at index z (fourier_covariant_sampler.py:78-86, init_specialization.py:196-214,
+// distributed_sampler.py:14-20).
+__device__ float2 init_value(const PassParams& P, u64 z) {
+  u64 b = 0, pm = 0;
+  if (P.init == INIT_PRODUCT) {
+    b = z;
+    pm = lut_parity_mask(P.lut_z, P.chunks, z);
+  } else {
+    const u64 marked = z | (1ull << 63);
+    for (int cc = 0; cc < P.chunks; ++cc) {
+      const u64* e = P.lut_z + ((((u64)cc << 8) + ((z >> (8 * cc)) & 255ull)) << 1);
+      b ^= __ldg(e);
+      pm ^= __ldg(e + 1) & marked;
+    }
+  }
+  double2 w;
+  if (P.init == INIT_COV_SPECIAL) {
+    w = __ldg(P.wspec + __popcll(b) * (P.m + 1) + __popcll(b & P.outmask));
+  } else {
+    w = __ldg(P.wgen + ((b & 255ull)));
+    for (int cc = 1; cc < P.chunks; ++cc) w = cmul(w, __ldg(P.wgen + ((u64)cc << 8) + ((b >> (8 * cc)) & 255ull)));
+  }
+  const float s = (__popcll(pm) & 1) ? -1.f : 1.f;
+  return make_float2(s * (float)w.x, s * (float)w.y);
+}
+
+__device__ __forceinline__ void apply_u(float2& x, float2& y, const double2* u4) {
+  const float2 a = make_float2((float)u4[0].x, (float)u4[0].y), b = make_float2((float)u4[1].x, (float)u4[1].y);
+  const float2 c = make_float2((float)u4[2].x, (float)u4[2].y), d = make_float2((float)u4[3].x, (float)u4[3].y);
+  const float2 nx = make_float2(a.x * x.x - a.y * x.y + b.x * y.x - b.y * y.y, a.x * x.y + a.y * x.x + b.x * y.y + b.y * y.x);
+  const float2 ny = make_float2(c.x * x.x - c.y * x.y + d.x * y.x - d.y * y.y, c.x * x.y + c.y * x.x + d.x * y.y + d.y * y.x);
+  x = nx;
+  y = ny;
+}
+
+// One four-axis round: registers hold the 16 elements whose tile-local bits
+// [w0, w0+4) vary; axes in `mask` (tile-local) get the WHT (wht) or their unitary.
+__device__ void tile_round(float2* sm, const PassParams& P, int TB, int w0, unsigned mask, bool wht) {
+  const int t = threadIdx.x;
+  const int f0 = ((t >> w0) << (w0 + 4)) | (t & ((1 << w0) - 1));
+  float2 r[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) r[i] = sm[swz(f0 | (i << w0))];
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    if (!((mask >> (w0 + a)) & 1u)) continue;
+    if (wht) {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        if (i & (1 << a)) continue;
+        const float2 x = r[i], y = r[i | (1 << a)];
+        r[i] = make_float2(x.x + y.x, x.y + y.y);
+        r[i | (1 << a)] = make_float2(x.x - y.x, x.y - y.y);
+      }
+    } else {
+      const double2* u4 = P.u + 4 * local_to_global_bit(P, w0 + a);
+      double2 uu[4] = {__ldg(u4), __ldg(u4 + 1), __ldg(u4 + 2), __ldg(u4 + 3)};
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        if (i & (1 << a)) continue;
+        apply_u(r[i], r[i | (1 << a)], uu);
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 16; ++i) sm[swz(f0 | (i << w0))] = r[i];
+  (void)TB;
+}
+
+__device__ void tile_rounds(float2* sm, const PassParams& P, int TB, unsigned mask, bool wht) {
+  for (int g0 = 0; g0 < TB; g0 += 4) {
+    const unsigned sel = mask & (((1u << min(4, TB - g0)) - 1u) << g0);
+    if (!sel) continue;
+    const int w0 = g0 + 4 <= TB ? g0 : TB - 4;
+    __syncthreads();
+    tile_round(sm, P, TB, w0, sel, wht);
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(512, 2) fourier_pass_kernel(const __grid_constant__ PassParams P) {
+  extern __shared__ float2 sm[];
+  const int TB = P.c + P.K;
+  const int nt = 1 << (TB - 4);
+  const u64 tile = blockIdx.x;
+  // Load (or compute) the tile.
+#pragma unroll 4
+  for (int k = 0; k < 16; ++k) {
+    const int f = threadIdx.x + k * nt;
+    const u64 g = tile_global(P, tile, f);
+    sm[swz(f)] = P.init ? init_value(P, g) : P.v[g];
+  }
+  if (P.wht_mask) tile_rounds(sm, P, TB, P.wht_mask, true);
+  if (P.phase) {
+    __syncthreads();
+    for (int k = 0; k < 16; ++k) {
+      const int f = threadIdx.x + k * nt;
+      const u64 g = tile_global(P, tile, f);
+      if (__popcll(lut_parity_mask(P.lut_a, P.chunks, g)) & 1) {
+        float2 x = sm[swz(f)];
+        sm[swz(f)] = make_float2(-x.x, -x.y);
+      }
+    }
+  }
+  if (P.u_mask) tile_rounds(sm, P, TB, P.u_mask, false);
+  __syncthreads();
+  double mass = 0.0;
+#pragma unroll 4
+  for (int k = 0; k < 16; ++k) {
+    const int f = threadIdx.x + k * nt;
+    const float2 x = sm[swz(f)];
+    if (P.store) P.v[tile_global(P, tile, f)] = x;
+    mass += (double)x.x * x.x + (double)x.y * x.y;
+  }
+  if (P.masses) {
+    __shared__ double red[32];
+    for (int off = 16; off; off >>= 1) mass += __shfl_xor_sync(0xffffffffu, mass, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mass;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < (nt + 31) / 32; ++w) s += red[w];
+      P.masses[tile] = s;
+    }
+  }
+}
+
+// Per-sample weight tables: generic chunk products over b (with 2^{-m/2} in chunk 0)
+// or the popcount table of identical B unitaries (init_specialization.py:98-115).
+__global__ void fourier_weights_kernel(int m, int chunks, const double2* __restrict__ uB, u64 outmask, int special,
+                                       double2* __restrict__ wgen, double2* __restrict__ wspec, int scale_half_m) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const double scale = scale_half_m ? exp2(-0.5 * m) : 1.0;
+  if (!special) {
+    if (e >= chunks * 256) return;
+    const int cc = e >> 8, code = e & 255;
+    double2 w = make_double2(cc == 0 ? scale : 1.0, 0.0);
+    for (int j = 8 * cc; j < min(m, 8 * cc + 8); ++j) {
+      const int bit = (code >> (j - 8 * cc)) & 1, out = (int)((outmask >> j) & 1ull);
+      w = cmul(w, uB[(j * 2 + out) * 2 + bit]);
+    }
+    wgen[e] = w;
+  } else {
+    if (e >= (m + 1) * (m + 1)) return;
+    const int k = e / (m + 1), h = e % (m + 1);
+    const int r = __popcll(outmask);
+    double2 w = make_double2(0.0, 0.0);
+    if (h >= max(0, r + k - m) && h <= min(r, k)) {
+      const int n[4] = {m - r - k + h, k - h, r - h, h};  // (out,b) = 00, 01, 10, 11
+      w = make_double2(scale, 0.0);
+      for (int t = 0; t < 4; ++t) {
+        const double2 base = uB[t];  // U_B[out][b] of site 0: flat order u00, u01, u10, u11
+        for (int p = 0; p < n[t]; ++p) w = cmul(w, base);
+      }
+    }
+    wspec[e] = w;
+  }
+}
+
+// Index map with q_A phase and scale (distributed_sampler.py:35-41), single device:
+// dst[z] = src[y(z)] (-1)^{q_A(z)} 2^{-m/2}, y = XOR_{k: z_k} cols[k].
+__global__ void fourier_index_map_kernel(const float2* __restrict__ src, float2* __restrict__ dst, int m, int chunks,
+                                         const u64* __restrict__ lut_cols, const u64* __restrict__ lut_a, float scale) {
+  const u64 n = 1ull << m;
+  for (u64 z = (u64)blockIdx.x * blockDim.x + threadIdx.x; z < n; z += (u64)gridDim.x * blockDim.x) {
+    u64 y = 0;
+    for (int cc = 0; cc < chunks; ++cc) y ^= __ldg(lut_cols + ((((u64)cc << 8) + ((z >> (8 * cc)) & 255ull)) << 1));
+    const float s = (__popcll(lut_parity_mask(lut_a, chunks, z)) & 1) ? -scale : scale;
+    const float2 x = src[y];
+    dst[z] = make_float2(s * x.x, s * x.y);
+  }
+}
+
+__global__ void block_mass_kernel(const float2* __restrict__ v, u64 n, int tile_bits, double* __restrict__ out) {
+  const u64 start = (u64)blockIdx.x << tile_bits;
+  const u64 end = min(n, start + (1ull << tile_bits));
+  double s = 0.0;
+  for (u64 i = start + threadIdx.x; i < end; i += blockDim.x) {
+    const float2 x = v[i];
+    s += (double)x.x * x.x + (double)x.y * x.y;
+  }
+  __shared__ double red[32];
+  for (int off = 16; off; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) t += red[w];
+    out[blockIdx.x] = t;
+  }
+}
+
+struct DrawResult {
+  unsigned long long index;
+  double pa, norm;
+  int status;
+};
+
+// First position i of v[0..n) with prefix(i) <= target < prefix(i) + v[i] (searchsorted
+// side='right' on the inclusive cumulative sum), found by one 1024-thread block.
+// Each thread sums a contiguous chunk; chunk sums are scanned in shared memory.
+template <class Get>
+__device__ long long block_search(long long n, double target, Get get, double* total_out) {
+  __shared__ double part[1024];
+  __shared__ long long found;
+  const int t = threadIdx.x, nt = blockDim.x;
+  const long long chunk = (n + nt - 1) / nt;
+  const long long lo = min(n, (long long)t * chunk), hi = min(n, lo + chunk);
+  double s = 0.0;
+  for (long long i = lo; i < hi; ++i) s += get(i);
+  part[t] = s;
+  if (t == 0) found = -1;
+  __syncthreads();
+  if (t == 0) {
+    double acc = 0.0;
+    for (int k = 0; k < nt; ++k) {
+      const double x = part[k];
+      part[k] = acc;
+      acc += x;
+    }
+    *total_out = acc;
+  }
+  __syncthreads();
+  const double pre = part[t];
+  if (pre <= target && target < pre + s) {
+    double acc = pre;
+    for (long long i = lo; i < hi; ++i) {
+      const double x = get(i);
+      if (target < acc + x) {
+        found = i;
+        break;
+      }
+      acc += x;
+    }
+  }
+  __syncthreads();
+  long long r = found;
+  __syncthreads();
+  if (r < 0) {  // target at/after the total (rounding): last non-zero entry
+    if (t == 0) {
+      for (long long i = n - 1; i >= 0; --i)
+        if (get(i) > 0.0) {
+          found = i;
+          break;
+        }
+    }
+    __syncthreads();
+    r = found;
+  }
+  return r;
+}
+
+__global__ void __launch_bounds__(1024) fourier_draw_kernel(const double* __restrict__ masses, long long ntiles,
+                                                            const float2* __restrict__ v, int m, int tile_bits,
+                                                            int deferred, const double2* __restrict__ uT,
+                                                            double u1, double u2, double u3,
+                                                            DrawResult* __restrict__ out) {
+  __shared__ double norm, tile_total;
+  double tot;
+  // First search (target 0) only establishes the total, then the draw itself.
+  block_search(ntiles, 0.0, [&](long long i) { return masses[i]; }, &tot);
+  if (threadIdx.x == 0) norm = tot;
+  __syncthreads();
+  const long long chosen = block_search(ntiles, u1 * norm, [&](long long i) { return masses[i]; }, &tot);
+  if (chosen < 0) {  // no tile with positive mass: report, read nothing
+    if (threadIdx.x == 0) {
+      DrawResult r{0ull, 0.0, norm, 2};
+      *out = r;
+    }
+    return;
+  }
+  const u64 base = (u64)chosen << tile_bits;
+  auto p_at = [&](long long i) {
+    const float2 x = v[base + (u64)i];
+    return (double)x.x * x.x + (double)x.y * x.y;
+  };
+  double tt;
+  block_search(1ll << tile_bits, 0.0, p_at, &tt);
+  if (threadIdx.x == 0) tile_total = tt;
+  __syncthreads();
+  const long long within = block_search(1ll << tile_bits, u2 * tile_total, p_at, &tt);
+  if (within < 0) {
+    if (threadIdx.x == 0) {
+      DrawResult r{0ull, 0.0, norm, 2};
+      *out = r;
+    }
+    return;
+  }
+  if (threadIdx.x == 0) {
+    const u64 idx = base + (u64)within;
+    DrawResult r;
+    r.norm = norm;
+    r.status = 0;
+    if (deferred) {
+      const u64 half = 1ull << (m - 1);
+      const u64 local = idx & (half - 1ull);
+      const float2 a = v[local], b = v[local + half];
+      const double2 A = make_double2(a.x, a.y), B = make_double2(b.x, b.y);
+      const double2 p0 = make_double2(cmul(uT[0], A).x + cmul(uT[1], B).x, cmul(uT[0], A).y + cmul(uT[1], B).y);
+      const double2 p1 = make_double2(cmul(uT[2], A).x + cmul(uT[3], B).x, cmul(uT[2], A).y + cmul(uT[3], B).y);
+      const double q0 = p0.x * p0.x + p0.y * p0.y, q1 = p1.x * p1.x + p1.y * p1.y;
+      const double total = q0 + q1;
+      if (!(total > 0.0) || !isfinite(total)) r.status = 1;
+      const int bit = (u3 * total >= q0) ? 1 : 0;
+      r.index = bit ? local + half : local;
+      r.pa = bit ? q1 : q0;
+    } else {
+      r.index = idx;
+      const float2 x = v[idx];
+      r.pa = (double)x.x * x.x + (double)x.y * x.y;
+    }
+    *out = r;
+  }
+}
+
+// ------------------------------------------------------------------------------------- host
+std::mutex g_fourier_mutex;
+
+int set_smem_attr() {
+  static bool done[64] = {false};
+  int device = 0;
+  RGS_CUDA_TRY(cudaGetDevice(&device));
+  std::lock_guard<std::mutex> lock(g_fourier_mutex);
+  if (device >= 0 && device < 64 && done[device]) return RGS_OK;
+  RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (1 << kTileBits) * (int)sizeof(float2)));
+  if (device >= 0 && device < 64) done[device] = true;
+  return RGS_OK;
+}
+
+int launch_pass(const PassParams& P, cudaStream_t s) {
+  const int TB = P.c + P.K;
+  if (TB < 4 || TB > kTileBits) return fail(RGS_ERR_UNSUPPORTED, "tile must span 4..13 bits");
+  const u64 tiles = 1ull << (P.m - TB);
+  int rc = set_smem_attr();
+  if (rc) return rc;
+  fourier_pass_kernel<<<(unsigned)tiles, 1 << (TB - 4), (1 << TB) * sizeof(float2), s>>>(P);
+  RGS_CUDA_TRY(cudaGetLastError());
+  return RGS_OK;
+}
+
+// Bit groups above the low tile: [kTileBits + 10 i, ...).
+std::vector<std::pair<int, int>> strided_groups(int m) {
+  std::vector<std::pair<int, int>> g;
+  for (int lo = kTileBits; lo < m; lo += kTileBits - kLowBits) g.push_back({lo, std::min(m, lo + kTileBits - kLowBits)});
+  return g;
+}
+
+PassParams base_params(const FourierPlan& p, float2* v) {
+  PassParams P{};
+  P.v = v;
+  P.m = p.m;
+  P.chunks = p.chunks;
+  P.lut_a = (const u64*)p.d_lut_a;
+  P.u = (const double2*)p.d_uA;
+  P.store = 1;
+  return P;
+}
+
+void contiguous(PassParams& P, int m) {
+  P.c = std::min(m, kTileBits);
+  P.K = 0;
+  P.q = P.c;
+}
+
+void strided(PassParams& P, int lo, int hi) {
+  P.c = kLowBits;
+  P.K = hi - lo;
+  P.q = lo;
+}
+
+unsigned target_mask(const PassParams& P) { return ((1u << P.K) - 1u) << P.c; }
+
+int local_to_global_host(const PassParams& P, int a) { return a < P.c ? a : P.q + (a - P.c); }
+
+// Product axes of a contiguous/strided tile, without the deferred terminal bit.
+unsigned product_mask(const FourierPlan& p, const PassParams& P, unsigned axes) {
+  if (!p.deferred) return axes;
+  for (int a = 0; a < P.c + P.K; ++a)
+    if (((axes >> a) & 1u) && local_to_global_host(P, a) == p.m - 1) axes &= ~(1u << a);
+  return axes;
+}
+
+// Passes applying `op` (WHT or products) to the bits [lo, hi) of an nbits state.
+int transform_range(PassParams P, int nbits, int lo, int hi, bool wht, cudaStream_t s) {
+  if (nbits < 4) return fail(RGS_ERR_UNSUPPORTED, "states of fewer than 4 qubits are not supported");
+  if (lo < 0 || hi > nbits || lo >= hi) return fail(RGS_ERR_ARG, "bad bit range");
+  P.m = nbits;
+  contiguous(P, nbits);
+  unsigned low = 0;
+  for (int b = lo; b < std::min(hi, P.c); ++b) low |= 1u << b;
+  if (low) {
+    P.wht_mask = wht ? low : 0;
+    P.u_mask = wht ? 0 : low;
+    int rc = launch_pass(P, s);
+    if (rc) return rc;
+  }
+  for (auto g : strided_groups(nbits)) {
+    const int a = std::max(lo, g.first), b = std::min(hi, g.second);
+    if (a >= b) continue;
+    strided(P, g.first, g.second);
+    unsigned mask = 0;
+    for (int bit = a; bit < b; ++bit) mask |= 1u << (P.c + bit - g.first);
+    P.wht_mask = wht ? mask : 0;
+    P.u_mask = wht ? 0 : mask;
+    int rc = launch_pass(P, s);
+    if (rc) return rc;
+  }
+  return RGS_OK;
+}
+
+int build_weights(FourierPlan& p, uint64_t outB, char* ws, const FourierLayout& L, bool special, bool scale,
+                  cudaStream_t s) {
+  double2* w = (double2*)(ws + L.off_weights);
+  const int entries = special ? (p.m + 1) * (p.m + 1) : p.chunks * 256;
+  fourier_weights_kernel<<<(entries + 255) / 256, 256, 0, s>>>(p.m, p.chunks, (const double2*)p.d_uB, outB,
+                                                               special ? 1 : 0, w, w, scale ? 1 : 0);
+  RGS_CUDA_TRY(cudaGetLastError());
+  return RGS_OK;
+}
+
+int check_state(FourierPlan& p, const void* state, void* ws, size_t ws_bytes, FourierLayout& L) {
+  if (!state || !ws) return fail(RGS_ERR_ARG, "null state or workspace");
+  if (((uintptr_t)state & 15) || ((uintptr_t)ws & 255)) return fail(RGS_ERR_ARG, "misaligned state or workspace");
+  fourier_layout(p, L);
+  if (ws_bytes < L.total) return fail(RGS_ERR_OOM, "workspace smaller than rgs_fourier_workspace_bytes()");
+  int device = 0;
+  int rc = bind_device_of(state, &device);
+  if (rc) return rc;
+  return fourier_upload(p, device);
+}
+
+}  // namespace
+
+std::string fourier_build(int n, const uint8_t* graph, const double* unitaries, int m, const int* A, const int* B,
+                          bool deferred, FourierPlan& p, int& status) {
+  status = RGS_ERR_ARG;
+  if (n < 2 || n > 128 || !graph || !unitaries || !A || !B) return "bad arguments";
+  if (m < 4 || m > 40) return "conditional size m must be in [4, 40]";
+  std::vector<char> seen(n, 0);
+  for (int j = 0; j < m; ++j) {
+    if (A[j] < 0 || A[j] >= n || B[j] < 0 || B[j] >= n) return "A/B vertex out of range";
+    if (seen[A[j]] || seen[B[j]] || A[j] == B[j]) return "A and B must be disjoint sets of distinct vertices";
+    seen[A[j]] = seen[B[j]] = 1;
+  }
+  auto g = [&](int a, int b) { return graph[(size_t)a * n + b] != 0; };
+  p.n = n;
+  p.m = m;
+  p.A.assign(A, A + m);
+  p.B.assign(B, B + m);
+  p.deferred = deferred;
+  std::vector<u64h> M(m, 0), gB(m, 0), gA(m, 0);
+  p.cols.assign(m, 0);
+  for (int j = 0; j < m; ++j)
+    for (int i = 0; i < m; ++i) {
+      if (g(B[j], A[i])) M[j] |= 1ull << i;
+      if (g(B[j], B[i])) gB[j] |= 1ull << i;
+      if (g(A[j], A[i])) gA[j] |= 1ull << i;
+      if (g(A[j], B[i])) p.cols[j] |= 1ull << i;
+    }
+  if (gf2_rank(M, m) != m) {
+    status = RGS_ERR_SINGULAR;
+    return "B marginal is not uniform: rank(G[B,A]) < |B|";
+  }
+  std::vector<u64h> inv;
+  if (!gf2_inverse(M, m, inv)) {
+    status = RGS_ERR_SINGULAR;
+    return "singular GF(2) matrix";
+  }
+  // N = inv^T: b_j = parity(row_j(N) & z); column j of N = row j of inv.
+  p.inv_rows = gf2_transpose(inv, m);
+  std::vector<u64h> Q;
+  u64h lin = 0;
+  transformed_quadratic(gB, p.inv_rows, m, Q, lin);
+  chunk_tables(m, kChunkBits, inv, Q, lin, p.lut_z, p.chunks);
+  p.qA = upper_masks(gA, m);
+  p.qB = upper_masks(gB, m);
+  int ch = 0;
+  chunk_tables(m, kChunkBits, {}, p.qA, 0, p.lut_a, ch);
+  chunk_tables(m, kChunkBits, p.cols, std::vector<u64h>(m, 0), 0, p.lut_cols, ch);
+  p.uA.resize((size_t)m * 8);
+  p.uB.resize((size_t)m * 8);
+  for (int j = 0; j < m; ++j)
+    for (int e = 0; e < 8; ++e) {
+      p.uA[(size_t)j * 8 + e] = unitaries[(size_t)A[j] * 8 + e];
+      p.uB[(size_t)j * 8 + e] = unitaries[(size_t)B[j] * 8 + e];
+    }
+  p.specialized = true;
+  for (int j = 1; j < m && p.specialized; ++j)
+    for (int e = 0; e < 8; ++e)
+      if (p.uB[(size_t)j * 8 + e] != p.uB[e]) p.specialized = false;
+  p.ngroups = (int)strided_groups(m).size();
+  status = RGS_OK;
+  return "";
+}
+
+void fourier_layout(const FourierPlan& p, FourierLayout& L) {
+  const int TB = std::min(p.m, kTileBits);
+  L.ntiles = 1ll << (p.m - TB);
+  L.off_masses = 0;
+  L.off_weights = align_up((size_t)L.ntiles * sizeof(double), 256);
+  const size_t wentries = std::max<size_t>((size_t)p.chunks * 256, (size_t)(p.m + 1) * (p.m + 1));
+  L.off_result = L.off_weights + align_up(wentries * 16, 256);
+  L.total = L.off_result + 256;
+}
+
+int fourier_upload(FourierPlan& p, int device) {
+  std::lock_guard<std::mutex> lock(g_fourier_mutex);
+  if (p.device == device) return RGS_OK;
+  if (p.device >= 0) return fail(RGS_ERR_ARG, "a conditional-sampler plan is bound to one device");
+  std::vector<u64h> bq;
+  int ch = 0;
+  chunk_tables(p.m, kChunkBits, {}, p.qB, 0, bq, ch);
+  // lut_z holds [covariant | q_B-over-b] back to back.
+  std::vector<u64h> z(p.lut_z);
+  z.insert(z.end(), bq.begin(), bq.end());
+  auto up = [&](void** dst, const void* src, size_t bytes) -> int {
+    RGS_CUDA_TRY(cudaMalloc(dst, bytes));
+    RGS_CUDA_TRY(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+    return RGS_OK;
+  };
+  int rc;
+  if ((rc = up(&p.d_lut_z, z.data(), z.size() * 8))) return rc;
+  if ((rc = up(&p.d_lut_a, p.lut_a.data(), p.lut_a.size() * 8))) return rc;
+  if ((rc = up(&p.d_lut_cols, p.lut_cols.data(), p.lut_cols.size() * 8))) return rc;
+  if ((rc = up(&p.d_uA, p.uA.data(), p.uA.size() * 8))) return rc;
+  if ((rc = up(&p.d_uB, p.uB.data(), p.uB.size() * 8))) return rc;
+  p.device = device;
+  return RGS_OK;
+}
+
+int fourier_compute(FourierPlan& p, uint64_t outB, void* state, void* ws, size_t ws_bytes, cudaStream_t s,
+                    FourierStages* stages) {
+  FourierLayout L;
+  int rc = check_state(p, state, ws, ws_bytes, L);
+  if (rc) return rc;
+  char* w = (char*)ws;
+  rc = build_weights(p, outB, w, L, p.specialized, true, s);
+  if (rc) return rc;
+  cudaEvent_t ev[4];
+  if (stages)
+    for (auto& e : ev) RGS_CUDA_TRY(cudaEventCreate(&e));
+  if (stages) RGS_CUDA_TRY(cudaEventRecord(ev[0], s));
+  PassParams P = base_params(p, (float2*)state);
+  P.init = p.specialized ? INIT_COV_SPECIAL : INIT_COV_GENERIC;
+  P.lut_z = (const u64*)p.d_lut_z;
+  P.wgen = (const double2*)(w + L.off_weights);
+  P.wspec = (const double2*)(w + L.off_weights);
+  P.outmask = outB;
+  double* masses = (double*)(w + L.off_masses);
+  const int m = p.m;
+  if (m <= kTileBits) {
+    contiguous(P, m);
+    P.wht_mask = (1u << m) - 1u;
+    P.phase = 1;
+    P.u_mask = product_mask(p, P, (1u << m) - 1u);
+    P.masses = masses;
+    if ((rc = launch_pass(P, s))) return rc;
+    if (stages) {
+      RGS_CUDA_TRY(cudaEventRecord(ev[1], s));
+      RGS_CUDA_TRY(cudaEventRecord(ev[2], s));
+    }
+  } else {
+    const auto groups = strided_groups(m);
+    const int k = (int)groups.size();
+    contiguous(P, m);
+    P.wht_mask = (1u << kTileBits) - 1u;
+    if ((rc = launch_pass(P, s))) return rc;
+    if (stages) RGS_CUDA_TRY(cudaEventRecord(ev[1], s));
+    P.init = INIT_LOAD;
+    for (int i = 0; i + 1 < k; ++i) {
+      strided(P, groups[i].first, groups[i].second);
+      P.wht_mask = target_mask(P);
+      if ((rc = launch_pass(P, s))) return rc;
+    }
+    strided(P, groups[k - 1].first, groups[k - 1].second);
+    P.wht_mask = target_mask(P);
+    P.phase = 1;
+    P.u_mask = product_mask(p, P, target_mask(P));
+    if ((rc = launch_pass(P, s))) return rc;
+    if (stages) RGS_CUDA_TRY(cudaEventRecord(ev[2], s));
+    P.phase = 0;
+    P.wht_mask = 0;
+    for (int i = k - 2; i >= 0; --i) {
+      strided(P, groups[i].first, groups[i].second);
+      P.u_mask = product_mask(p, P, target_mask(P));
+      if ((rc = launch_pass(P, s))) return rc;
+    }
+    contiguous(P, m);
+    P.u_mask = product_mask(p, P, (1u << kTileBits) - 1u);
+    P.masses = masses;
+    if ((rc = launch_pass(P, s))) return rc;
+  }
+  if (stages) {
+    RGS_CUDA_TRY(cudaEventRecord(ev[3], s));
+    RGS_CUDA_TRY(cudaEventSynchronize(ev[3]));
+    cudaEventElapsedTime(&stages->init_ms, ev[0], ev[1]);
+    cudaEventElapsedTime(&stages->walsh_ms, ev[1], ev[2]);
+    cudaEventElapsedTime(&stages->product_ms, ev[2], ev[3]);
+    for (auto& e : ev) cudaEventDestroy(e);
+  }
+  return RGS_OK;
+}
+
+int fourier_compute_permute(FourierPlan& p, uint64_t outB, void* state, void* scratch, void* ws, size_t ws_bytes,
+                            cudaStream_t s) {
+  FourierLayout L;
+  int rc = check_state(p, state, ws, ws_bytes, L);
+  if (rc) return rc;
+  if (!scratch || ((uintptr_t)scratch & 15)) return fail(RGS_ERR_ARG, "bad scratch state");
+  char* w = (char*)ws;
+  rc = build_weights(p, outB, w, L, false, false, s);
+  if (rc) return rc;
+  const int m = p.m;
+  PassParams P = base_params(p, (float2*)state);
+  P.init = INIT_PRODUCT;
+  P.lut_z = (const u64*)p.d_lut_z + (size_t)p.chunks * 256 * 2;  // q_B over b
+  P.wgen = (const double2*)(w + L.off_weights);
+  contiguous(P, m);
+  P.wht_mask = (1u << P.c) - 1u;
+  if ((rc = launch_pass(P, s))) return rc;
+  P.init = INIT_LOAD;
+  if (m > kTileBits && (rc = transform_range(P, m, kTileBits, m, true, s))) return rc;
+  const u64 n = 1ull << m;
+  const unsigned blocks = (unsigned)std::min<u64>((n + 255) / 256, (u64)sm_count(p.device) * 32);
+  fourier_index_map_kernel<<<blocks, 256, 0, s>>>((const float2*)state, (float2*)scratch, m, p.chunks,
+                                                  (const u64*)p.d_lut_cols, (const u64*)p.d_lut_a,
+                                                  (float)std::exp2(-0.5 * m));
+  RGS_CUDA_TRY(cudaGetLastError());
+  PassParams Q = base_params(p, (float2*)scratch);
+  // Products on all bits but the deferred terminal one, then the masses.
+  const int top = p.deferred ? m - 1 : m;
+  if (top > std::min(m, kTileBits) && (rc = transform_range(Q, m, std::min(m, kTileBits), top, false, s))) return rc;
+  contiguous(Q, m);
+  Q.u_mask = product_mask(p, Q, (1u << Q.c) - 1u);
+  Q.masses = (double*)(w + L.off_masses);
+  return launch_pass(Q, s);
+}
+
+int fourier_masses(FourierPlan& p, const void* state, void* ws, cudaStream_t s) {
+  FourierLayout L;
+  int rc = check_state(p, state, ws, (size_t)-1, L);
+  if (rc) return rc;
+  return block_mass(state, p.m, std::min(p.m, kTileBits), (double*)((char*)ws + L.off_masses), s);
+}
+
+int fourier_draw(FourierPlan& p, const void* state, void* ws, double u1, double u2, double u3, uint64_t* index,
+                 double* pa, double* norm, cudaStream_t s) {
+  FourierLayout L;
+  int rc = check_state(p, state, ws, (size_t)-1, L);
+  if (rc) return rc;
+  if (!(u1 >= 0.0 && u1 < 1.0 && u2 >= 0.0 && u2 < 1.0 && u3 >= 0.0 && u3 < 1.0))
+    return fail(RGS_ERR_ARG, "uniforms must lie in [0, 1)");
+  char* w = (char*)ws;
+  DrawResult* d = (DrawResult*)(w + L.off_result);
+  fourier_draw_kernel<<<1, 1024, 0, s>>>((const double*)(w + L.off_masses), L.ntiles, (const float2*)state, p.m,
+                                         std::min(p.m, kTileBits), p.deferred ? 1 : 0,
+                                         (const double2*)p.d_uA + 4 * (p.m - 1), u1, u2, u3, d);
+  RGS_CUDA_TRY(cudaGetLastError());
+  DrawResult h;
+  RGS_CUDA_TRY(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, s));
+  RGS_CUDA_TRY(cudaStreamSynchronize(s));
+  if (!std::isfinite(h.norm) || std::fabs(h.norm - 1.0) > 1e-3)
+    return fail(RGS_ERR_ZERO_NORM, "conditional norm check failed: " + std::to_string(h.norm));
+  if (h.status || !(h.pa > 0.0) || !std::isfinite(h.pa)) return fail(RGS_ERR_NONFINITE, "invalid drawn probability");
+  *index = h.index;
+  *pa = h.pa;
+  *norm = h.norm;
+  return RGS_OK;
+}
+
+int fourier_index_map(FourierPlan& p, const void* src, void* dst, cudaStream_t s) {
+  if (!src || !dst || src == dst) return fail(RGS_ERR_ARG, "index map needs distinct source and destination");
+  int device = 0;
+  int rc = bind_device_of(dst, &device);
+  if (rc) return rc;
+  if ((rc = fourier_upload(p, device))) return rc;
+  const u64 n = 1ull << p.m;
+  const unsigned blocks = (unsigned)std::min<u64>((n + 255) / 256, (u64)sm_count(device) * 32);
+  fourier_index_map_kernel<<<blocks, 256, 0, s>>>((const float2*)src, (float2*)dst, p.m, p.chunks,
+                                                  (const u64*)p.d_lut_cols, (const u64*)p.d_lut_a,
+                                                  (float)std::exp2(-0.5 * p.m));
+  RGS_CUDA_TRY(cudaGetLastError());
+  return RGS_OK;
+}
+
+int fourier_quadphase(FourierPlan& p, void* state, cudaStream_t s) {
+  int device = 0;
+  int rc = bind_device_of(state, &device);
+  if (rc) return rc;
+  if ((rc = fourier_upload(p, device))) return rc;
+  PassParams P = base_params(p, (float2*)state);
+  contiguous(P, p.m);
+  P.phase = 1;
+  return launch_pass(P, s);
+}
+
+int fwht_bits(void* state, int nbits, int lo, int hi, cudaStream_t s) {
+  int device = 0;
+  int rc = bind_device_of(state, &device);
+  if (rc) return rc;
+  PassParams P{};
+  P.v = (float2*)state;
+  P.store = 1;
+  return transform_range(P, nbits, lo, hi, true, s);
+}
+
+int product_bits(void* state, int nbits, const double* u_dev, int lo, int hi, cudaStream_t s) {
+  int device = 0;
+  int rc = bind_device_of(state, &device);
+  if (rc) return rc;
+  if (!u_dev) return fail(RGS_ERR_ARG, "unitaries are required");
+  PassParams P{};
+  P.v = (float2*)state;
+  P.store = 1;
+  P.u = (const double2*)u_dev;
+  return transform_range(P, nbits, lo, hi, false, s);
+}
+
+int block_mass(const void* state, int nbits, int tile_bits, double* masses, cudaStream_t s) {
+  if (!state || !masses || nbits < 0 || nbits > 40 || tile_bits < 0 || tile_bits > nbits)
+    return fail(RGS_ERR_ARG, "bad block-mass arguments");
+  const u64 n = 1ull << nbits;
+  const unsigned blocks = (unsigned)(n >> tile_bits);
+  block_mass_kernel<<<blocks, 256, 0, s>>>((const float2*)state, n, tile_bits, masses);
+  RGS_CUDA_TRY(cudaGetLastError());
+  return RGS_OK;
+}
+
+}  // namespace rgs

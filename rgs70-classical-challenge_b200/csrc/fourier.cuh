@@ -1,0 +1,82 @@
+// Conditional (Fourier-cut) sampler: host-side plan and kernel entry points.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "gf2.hpp"
+
+namespace rgs {
+
+constexpr int kTileBits = 13;   // elements per tile = 2^13 (64 KiB of complex64 in shared memory)
+constexpr int kLowBits = 3;     // contiguous low bits kept in strided tiles (64-byte runs)
+constexpr int kChunkBits = 8;   // lookup-table chunk width over z (init_specialization.py:160)
+
+struct FourierPlan {
+  int n = 0, m = 0;
+  std::vector<int> A, B;
+  bool specialized = false;      // all U_B identical: popcount weight table (init_specialization.py)
+  bool deferred = true;          // terminal unitary on bit m-1 applied at draw time
+  int chunks = 0;
+  std::vector<u64h> lut_z;       // [chunks][256][2] covariant map + transformed q_B
+  std::vector<u64h> lut_a;       // [chunks][256][2] q_A phase (entry[0] = 0)
+  std::vector<u64h> lut_cols;    // [chunks][256][2] index map of the permutation path
+  std::vector<u64h> inv_rows;    // rows of N = M^{-T} (b_j = parity(N_j & z))
+  std::vector<u64h> qB, qA;      // strict-upper masks of g_BB, g_AA (distributed_sampler.py:57)
+  std::vector<u64h> cols;        // cols[k] = mask over B of g[A_k, B] (distributed_sampler.py:68)
+  std::vector<double> uA, uB;    // complex128 [m][2][2] of the A / B sites
+  // Pass schedule (see fourier.cu).
+  int ngroups = 0;               // strided target groups above the low tile
+  // Device copies.
+  int device = -1;
+  void* d_lut_z = nullptr;
+  void* d_lut_a = nullptr;
+  void* d_lut_cols = nullptr;
+  void* d_uA = nullptr;          // complex64 [m][2][2]
+  void* d_uB = nullptr;          // complex128 [m][2][2]
+  ~FourierPlan();
+};
+
+// Workspace: per-tile masses (double), per-sample weight tables, draw result.
+struct FourierLayout {
+  size_t off_masses = 0, off_weights = 0, off_result = 0, total = 0;
+  long long ntiles = 0;
+};
+
+std::string fourier_build(int n, const uint8_t* graph, const double* unitaries, int m, const int* A, const int* B,
+                          bool deferred, FourierPlan& p, int& status);
+void fourier_layout(const FourierPlan& p, FourierLayout& L);
+int fourier_upload(FourierPlan& p, int device);
+
+struct FourierStages {
+  float init_ms = 0, walsh_ms = 0, product_ms = 0;
+};
+
+// Full conditional state for outcome mask outB (bit j = outcome of B_j), in place in
+// `state` (complex64[2^m]); tile masses into the workspace.  If `stages` is given the
+// call synchronises and reports device time per stage.
+int fourier_compute(FourierPlan& p, uint64_t outB, void* state, void* ws, size_t ws_bytes, cudaStream_t s,
+                    FourierStages* stages);
+// Reference pipeline (W/distributed_sampler.py:126-144, single device): product init over
+// b, WHT, index map with q_A phase into `scratch`, products; result in `scratch`.
+int fourier_compute_permute(FourierPlan& p, uint64_t outB, void* state, void* scratch, void* ws, size_t ws_bytes,
+                            cudaStream_t s);
+// Tile masses of a state (no transform), for states produced elsewhere.
+int fourier_masses(FourierPlan& p, const void* state, void* ws, cudaStream_t s);
+// Two-level inverse CDF + terminal pair (deferred_global_sampler.py:65-78); synchronises.
+int fourier_draw(FourierPlan& p, const void* state, void* ws, double u1, double u2, double u3, uint64_t* index,
+                 double* pa, double* norm, cudaStream_t s);
+
+// dst[z] = src[y(z)] (-1)^{q_A(z)} 2^{-m/2}, y = XOR_{k: z_k} cols[k] (distributed_sampler.py:35-41).
+int fourier_index_map(FourierPlan& p, const void* src, void* dst, cudaStream_t s);
+// state[z] *= (-1)^{q_A(z)} (graph_sampler.py:76-85 on the A vertices).
+int fourier_quadphase(FourierPlan& p, void* state, cudaStream_t s);
+
+// Building blocks on a state of 2^nbits complex64 values (in place).
+int fwht_bits(void* state, int nbits, int lo, int hi, cudaStream_t s);
+int product_bits(void* state, int nbits, const double* u_host, int lo, int hi, cudaStream_t s);
+int block_mass(const void* state, int nbits, int tile_bits, double* masses, cudaStream_t s);
+
+}  // namespace rgs

@@ -27,8 +27,6 @@ int scan_layout(const Plan& plan, int Bt, int precision, ScanLayout& L);
 // Largest batch tile the step kernel supports for a precision.
 int scan_max_tile(int precision);
 
-// Makes the device owning `p` current for this library's runtime and returns it.
-int bind_device_of(const void* p, int* device);
 
 // Uploads (once per device) the plan's step records, byte tables and vertex records.
 int plan_device_copy(Plan& plan, int device, const Plan::DeviceCopy** out);

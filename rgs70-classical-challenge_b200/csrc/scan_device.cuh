@@ -20,10 +20,21 @@ struct Cx {
   M re, im;
 };
 
+// acc += e * w with an explicit fused-multiply-add order, so the result of an item
+// does not depend on how the compiler schedules a particular kernel instantiation
+// (batch tiles of every size give bitwise-identical amplitudes).
 template <typename M>
 __device__ __forceinline__ void cmad(Cx<M>& acc, M er, M ei, const Cx<M>& w) {
-  acc.re += er * w.re - ei * w.im;
-  acc.im += er * w.im + ei * w.re;
+  acc.re = fma(er, w.re, acc.re);
+  acc.re = fma(-ei, w.im, acc.re);
+  acc.im = fma(er, w.im, acc.im);
+  acc.im = fma(ei, w.re, acc.im);
+}
+
+// |x|^2 with a fixed rounding sequence.
+template <typename S>
+__device__ __forceinline__ S norm2(S re, S im) {
+  return fma(re, re, im * im);
 }
 
 // One 16-byte (or, for single-item complex64 rows, 8-byte) chunk of a table row:

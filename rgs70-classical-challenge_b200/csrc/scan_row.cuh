@@ -176,11 +176,11 @@ __global__ void __launch_bounds__(256, 2) scan_row_kernel(const S* __restrict__ 
           }
           const S ar = (S)oa.re, ai = (S)oa.im;
           outA.set(v, ar, ai);
-          mx[i] = fmax(mx[i], ar * ar + ai * ai);
+          mx[i] = fmax(mx[i], norm2(ar, ai));
           if (MODE == MODE_PAIR) {
             const S br = (S)ob.re, bi = (S)ob.im;
             outB.set(v, br, bi);
-            mx[i] = fmax(mx[i], br * br + bi * bi);
+            mx[i] = fmax(mx[i], norm2(br, bi));
           }
         }
         const u64 col = (u64)(l + (j << lL));
