@@ -338,6 +338,76 @@ def run_ours(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def fourier_instance(pkg, m, seed=None):
+    """Seeded dense graph on 2m vertices with a full-rank balanced cut A = 0..m-1,
+    B = m..2m-1; Haar gates, identical on B (the reference's production specialisation)."""
+    rng = np.random.default_rng(1000 + m if seed is None else seed)
+    while True:
+        g = pkg.instances.dense(2 * m, rng)
+        A, B = list(range(m)), list(range(m, 2 * m))
+        try:
+            pkg.samplers.cut_tables(g, np.tile(np.eye(2, dtype=np.complex128), (2 * m, 1, 1)), A, B)
+            break
+        except ValueError:
+            continue
+    u = pkg.instances.haar_su2(2 * m, rng)
+    u[B] = u[B[0]]
+    return g, u, A, B
+
+
+def run_fourier(args, rank, world, local_rank):
+    """One step = one exact conditional Born sample (compute + draw) of the Fourier-cut
+    sampler at m conditional qubits (2^m complex64 state on one GPU)."""
+    import ctypes
+    import torch
+    import __graft_entry__
+    pkg = __graft_entry__.package()
+    device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+    m = args.m
+    g, u, A, B = fourier_instance(pkg, m)
+    s = pkg.ConditionalSampler(g, u, A, B, [local_rank])
+    L = pkg._lib.lib()
+    stream = torch.cuda.current_stream(device)
+    rng = np.random.default_rng(99 + rank)
+
+    def sample():
+        ob = rng.integers(0, 2, m)
+        mask = int(sum(int(x) << j for j, x in enumerate(ob)))
+        pkg._lib.check(L.rgs_fourier_compute(s._h, mask, ctypes.c_void_p(s.state.data_ptr()),
+                                             ctypes.c_void_p(s.workspace.data_ptr()), s.workspace.numel(),
+                                             ctypes.c_void_p(stream.cuda_stream), None))
+        return s.draw(rng)
+
+    for _ in range(args.warmup):
+        sample()
+    torch.cuda.synchronize(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            sample()
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+    t = e0.elapsed_time(e1) / 1e3
+    groups = 0 if m <= 13 else -(-(m - 13) // 10)
+    bytes_per_sample = (1 << m) * (8 + 16 * 2 * groups)
+    peak = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]) \
+        if (ROOT / "MEASURED_PEAKS.json").exists() else 6650.0
+    achieved = bytes_per_sample * args.steps / t / 1e9
+    if rank == 0:
+        print(json.dumps({
+            "metric": f"exact_born_samples_per_s (Fourier-cut conditional sampler, m={m})",
+            "value": args.steps / t, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded dense graph)",
+            "config": {"workload": f"conditional sampler, dense graph n={2 * m}, full-rank balanced cut m={m}",
+                       "passes": s.passes, "specialized": s.specialized},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "algorithmic_bytes_per_step": bytes_per_sample},
+            "gpu_launches": args.steps * (s.passes + 2), "clocks": clocks.summary()}), flush=True)
+
+
 def main():
     global BATCH
     ap = argparse.ArgumentParser()
@@ -350,6 +420,8 @@ def main():
     ap.add_argument("--only", choices=["both", "c64", "c128"], default="both",
                     help="run only one precision (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--workload", choices=["amplitudes", "fourier"], default="amplitudes")
+    ap.add_argument("--m", type=int, default=30, help="conditional qubits of the fourier workload")
     ap.add_argument("--tile64", type=int, default=128)
     ap.add_argument("--tile128", type=int, default=64)
     args = ap.parse_args()
@@ -361,6 +433,8 @@ def main():
     BATCH = args.batch
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.workload == "fourier":
+        run_fourier(args, rank, world, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
 

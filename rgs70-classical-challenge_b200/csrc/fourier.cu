@@ -10,18 +10,22 @@
 // distributed_sampler.py:50-54, 145-157; deferred_global_sampler.py:65-78).
 //
 // Pass structure.  The state is 2^m complex64 values in HBM.  A pass streams it once
-// in tiles of 2^13 elements staged in shared memory: either a contiguous tile (the 13
-// low bits) or a strided tile (3 contiguous low bits = 64-byte runs, times up to 10
-// "target" bits at position q).  Inside a tile each thread holds 16 elements in
+// in tiles of 2^12 elements staged in shared memory (four 256-thread blocks per SM):
+// either a contiguous tile (the 12 low bits) or a strided tile (at least 3 contiguous
+// low bits = 64-byte runs, times up to 9 "target" bits at position q).  Inside a tile each thread holds 16 elements in
 // registers along 4 tile axes and applies every 2x2 operation on those axes; four-axis
 // rounds are separated by a swizzled shared-memory exchange.  The whole transform is
-//   pass 0          : init (computed, not loaded) + WHT on bits [0, 13)
-//   strided passes  : WHT on the next groups of 10 bits
+//   pass 0          : init (computed, not loaded) + WHT on bits [0, 12)
+//   strided passes  : WHT on the next groups of <= 9 bits (balanced)
 //   middle pass     : WHT on the last group, q_A phase, products on that group
 //   strided passes  : products on the earlier groups (reverse order)
-//   last pass       : products on bits [0, 13) + per-tile masses (float64)
-// = 2k+1 passes for m = 13 + 10k bits: 8 + 16*2k bytes per element (the reference
+//   last pass       : products on bits [0, 12) + per-tile masses (float64)
+// = 2k+1 passes with k = ceil((m-12)/9): 8 + 16*2k bytes per element (the reference
 // streams 2 + 2*ceil((m-10)/5) passes of 16 bytes, plus a mass pass).
+//
+// Lookup tables (init and phase) are evaluated per element only for the 8-bit chunks
+// of z that vary inside the tile; the chunks that are constant over a tile are folded
+// into per-tile constants once (parity is linear: XOR_c (x_c & z) = (XOR_c x_c) & z).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -90,21 +94,49 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// Initial value at index z (fourier_covariant_sampler.py:78-86, init_specialization.py:196-214,
-// distributed_sampler.py:14-20).
-__device__ float2 init_value(const PassParams& P, u64 z) {
-  u64 b = 0, pm = 0;
-  if (P.init == INIT_PRODUCT) {
-    b = z;
-    pm = lut_parity_mask(P.lut_z, P.chunks, z);
-  } else {
-    const u64 marked = z | (1ull << 63);
-    for (int cc = 0; cc < P.chunks; ++cc) {
-      const u64* e = P.lut_z + ((((u64)cc << 8) + ((z >> (8 * cc)) & 255ull)) << 1);
-      b ^= __ldg(e);
-      pm ^= __ldg(e + 1) & marked;
+// Chunk lookups that are constant over a tile, folded once per tile: b and the
+// phase mask of every chunk whose 8 bits of z do not vary in the tile.
+struct TileLut {
+  u64 b_const, pm_const;
+  unsigned var;  // bit c: chunk c varies in the tile
+  int chunks;
+};
+
+__device__ __forceinline__ void tile_lut(const u64* lut, int chunks, u64 base, u64 varying, TileLut& t) {
+  t.b_const = 0;
+  t.pm_const = 0;
+  t.var = 0;
+  t.chunks = chunks;
+  for (int cc = 0; cc < chunks; ++cc) {
+    if ((varying >> (8 * cc)) & 255ull) {
+      t.var |= 1u << cc;
+    } else {
+      const u64* e = lut + ((((u64)cc << 8) + ((base >> (8 * cc)) & 255ull)) << 1);
+      t.b_const ^= __ldg(e);
+      t.pm_const ^= __ldg(e + 1);
     }
   }
+}
+
+// (b, phase-parity mask) of z from the varying chunks plus the tile constants.
+__device__ __forceinline__ void tile_lut_eval(const u64* lut, const TileLut& t, u64 z, u64& b, u64& pm) {
+  b = t.b_const;
+  pm = t.pm_const;
+  for (int cc = 0; cc < t.chunks; ++cc) {
+    if (!((t.var >> cc) & 1u)) continue;
+    const u64* e = lut + ((((u64)cc << 8) + ((z >> (8 * cc)) & 255ull)) << 1);
+    b ^= __ldg(e);
+    pm ^= __ldg(e + 1);
+  }
+  pm &= z | (1ull << 63);
+}
+
+// Initial value at index z (fourier_covariant_sampler.py:78-86, init_specialization.py:196-214,
+// distributed_sampler.py:14-20).  For INIT_PRODUCT the table has no map part (b = z).
+__device__ float2 init_value(const PassParams& P, const TileLut& t, u64 z) {
+  u64 b, pm;
+  tile_lut_eval(P.lut_z, t, z, b, pm);
+  if (P.init == INIT_PRODUCT) b = z;
   double2 w;
   if (P.init == INIT_COV_SPECIAL) {
     w = __ldg(P.wspec + __popcll(b) * (P.m + 1) + __popcll(b & P.outmask));
@@ -116,11 +148,11 @@ __device__ float2 init_value(const PassParams& P, u64 z) {
   return make_float2(s * (float)w.x, s * (float)w.y);
 }
 
-__device__ __forceinline__ void apply_u(float2& x, float2& y, const double2* u4) {
-  const float2 a = make_float2((float)u4[0].x, (float)u4[0].y), b = make_float2((float)u4[1].x, (float)u4[1].y);
-  const float2 c = make_float2((float)u4[2].x, (float)u4[2].y), d = make_float2((float)u4[3].x, (float)u4[3].y);
-  const float2 nx = make_float2(a.x * x.x - a.y * x.y + b.x * y.x - b.y * y.y, a.x * x.y + a.y * x.x + b.x * y.y + b.y * y.x);
-  const float2 ny = make_float2(c.x * x.x - c.y * x.y + d.x * y.x - d.y * y.y, c.x * x.y + c.y * x.x + d.x * y.y + d.y * y.x);
+__device__ __forceinline__ void apply_u(float2& x, float2& y, const float2 (&u)[4]) {
+  const float2 nx = make_float2(u[0].x * x.x - u[0].y * x.y + u[1].x * y.x - u[1].y * y.y,
+                                u[0].x * x.y + u[0].y * x.x + u[1].x * y.y + u[1].y * y.x);
+  const float2 ny = make_float2(u[2].x * x.x - u[2].y * x.y + u[3].x * y.x - u[3].y * y.y,
+                                u[2].x * x.y + u[2].y * x.x + u[3].x * y.y + u[3].y * y.x);
   x = nx;
   y = ny;
 }
@@ -146,7 +178,12 @@ __device__ void tile_round(float2* sm, const PassParams& P, int TB, int w0, unsi
       }
     } else {
       const double2* u4 = P.u + 4 * local_to_global_bit(P, w0 + a);
-      double2 uu[4] = {__ldg(u4), __ldg(u4 + 1), __ldg(u4 + 2), __ldg(u4 + 3)};
+      float2 uu[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const double2 d = __ldg(u4 + e);
+        uu[e] = make_float2((float)d.x, (float)d.y);
+      }
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
         if (i & (1 << a)) continue;
@@ -159,50 +196,84 @@ __device__ void tile_round(float2* sm, const PassParams& P, int TB, int w0, unsi
   (void)TB;
 }
 
+// Four-axis rounds covering every axis of `mask`: each window starts at the lowest
+// axis not yet applied (clipped to the tile), so K target bits take ceil(K/4) rounds.
 __device__ void tile_rounds(float2* sm, const PassParams& P, int TB, unsigned mask, bool wht) {
-  for (int g0 = 0; g0 < TB; g0 += 4) {
-    const unsigned sel = mask & (((1u << min(4, TB - g0)) - 1u) << g0);
-    if (!sel) continue;
-    const int w0 = g0 + 4 <= TB ? g0 : TB - 4;
+  while (mask) {
+    const int a = __ffs(mask) - 1;
+    const int w0 = a + 4 <= TB ? a : TB - 4;
+    const unsigned sel = mask & (15u << w0);
     __syncthreads();
     tile_round(sm, P, TB, w0, sel, wht);
+    mask &= ~sel;
   }
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(512, 2) fourier_pass_kernel(const __grid_constant__ PassParams P) {
+__global__ void __launch_bounds__(256, 3) fourier_pass_kernel(const __grid_constant__ PassParams P) {
   extern __shared__ float2 sm[];
   const int TB = P.c + P.K;
   const int nt = 1 << (TB - 4);
   const u64 tile = blockIdx.x;
-  // Load (or compute) the tile.
-#pragma unroll 4
-  for (int k = 0; k < 16; ++k) {
-    const int f = threadIdx.x + k * nt;
-    const u64 g = tile_global(P, tile, f);
-    sm[swz(f)] = P.init ? init_value(P, g) : P.v[g];
+  const u64 base = tile_global(P, tile, 0);
+  const u64 varying = ((1ull << P.c) - 1ull) | (((1ull << P.K) - 1ull) << P.q);
+  // Load (or compute) the tile: each thread owns 8 element pairs (16-byte accesses,
+  // pairs are adjacent in memory because tile bit 0 is a contiguous bit).
+  if (P.init) {
+    TileLut t;
+    tile_lut(P.lut_z, P.chunks, base, varying, t);
+#pragma unroll 2
+    for (int k = 0; k < 8; ++k) {
+      const int f = 2 * (threadIdx.x + k * nt);
+      const u64 g = tile_global(P, tile, f);
+      sm[swz(f)] = init_value(P, t, g);
+      sm[swz(f + 1)] = init_value(P, t, g + 1);
+    }
+  } else {
+#pragma unroll
+    for (int h = 0; h < 8; h += 4) {
+      float4 x[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int f = 2 * (threadIdx.x + (h + k) * nt);
+        x[k] = *reinterpret_cast<const float4*>(P.v + tile_global(P, tile, f));
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int f = 2 * (threadIdx.x + (h + k) * nt);
+        sm[swz(f)] = make_float2(x[k].x, x[k].y);
+        sm[swz(f + 1)] = make_float2(x[k].z, x[k].w);
+      }
+    }
   }
   if (P.wht_mask) tile_rounds(sm, P, TB, P.wht_mask, true);
   if (P.phase) {
+    TileLut t;
+    tile_lut(P.lut_a, P.chunks, base, varying, t);
     __syncthreads();
-    for (int k = 0; k < 16; ++k) {
-      const int f = threadIdx.x + k * nt;
+    for (int k = 0; k < 8; ++k) {
+      const int f = 2 * (threadIdx.x + k * nt);
       const u64 g = tile_global(P, tile, f);
-      if (__popcll(lut_parity_mask(P.lut_a, P.chunks, g)) & 1) {
-        float2 x = sm[swz(f)];
-        sm[swz(f)] = make_float2(-x.x, -x.y);
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        u64 b, pm;
+        tile_lut_eval(P.lut_a, t, g + e, b, pm);
+        if (__popcll(pm) & 1) {
+          const float2 x = sm[swz(f + e)];
+          sm[swz(f + e)] = make_float2(-x.x, -x.y);
+        }
       }
     }
   }
   if (P.u_mask) tile_rounds(sm, P, TB, P.u_mask, false);
   __syncthreads();
   double mass = 0.0;
-#pragma unroll 4
-  for (int k = 0; k < 16; ++k) {
-    const int f = threadIdx.x + k * nt;
-    const float2 x = sm[swz(f)];
-    if (P.store) P.v[tile_global(P, tile, f)] = x;
-    mass += (double)x.x * x.x + (double)x.y * x.y;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int f = 2 * (threadIdx.x + k * nt);
+    const float2 a = sm[swz(f)], b = sm[swz(f + 1)];
+    if (P.store) *reinterpret_cast<float4*>(P.v + tile_global(P, tile, f)) = make_float4(a.x, a.y, b.x, b.y);
+    mass += (double)a.x * a.x + (double)a.y * a.y + (double)b.x * b.x + (double)b.y * b.y;
   }
   if (P.masses) {
     __shared__ double red[32];
@@ -431,10 +502,20 @@ int launch_pass(const PassParams& P, cudaStream_t s) {
   return RGS_OK;
 }
 
-// Bit groups above the low tile: [kTileBits + 10 i, ...).
+// Bit groups above the low tile, as equal as possible and at most 10 bits each
+// (a strided tile keeps at least 3 contiguous low bits = 64-byte runs).
 std::vector<std::pair<int, int>> strided_groups(int m) {
   std::vector<std::pair<int, int>> g;
-  for (int lo = kTileBits; lo < m; lo += kTileBits - kLowBits) g.push_back({lo, std::min(m, lo + kTileBits - kLowBits)});
+  const int rest = m - kTileBits;
+  if (rest <= 0) return g;
+  const int maxk = kTileBits - kLowBits;
+  const int k = (rest + maxk - 1) / maxk;
+  int lo = kTileBits;
+  for (int i = 0; i < k; ++i) {
+    const int size = rest / k + (i < rest % k ? 1 : 0);
+    g.push_back({lo, lo + size});
+    lo += size;
+  }
   return g;
 }
 
@@ -455,9 +536,11 @@ void contiguous(PassParams& P, int m) {
   P.q = P.c;
 }
 
+// A strided tile spans 13 bits: the target bits [lo, hi) plus as many contiguous low
+// bits as fit (longer runs when the group is small).
 void strided(PassParams& P, int lo, int hi) {
-  P.c = kLowBits;
   P.K = hi - lo;
+  P.c = kTileBits - P.K;
   P.q = lo;
 }
 

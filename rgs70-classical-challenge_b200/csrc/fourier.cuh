@@ -10,7 +10,7 @@
 
 namespace rgs {
 
-constexpr int kTileBits = 13;   // elements per tile = 2^13 (64 KiB of complex64 in shared memory)
+constexpr int kTileBits = 12;   // elements per tile = 2^12 (32 KiB of complex64 in shared memory)
 constexpr int kLowBits = 3;     // contiguous low bits kept in strided tiles (64-byte runs)
 constexpr int kChunkBits = 8;   // lookup-table chunk width over z (init_specialization.py:160)
 
