@@ -71,7 +71,10 @@ struct PassParams {
   int store;
 };
 
-__device__ __forceinline__ int swz(int f) { return f ^ ((f >> 4) & 15); }
+// Padded shared-memory layout: one spare slot per 16 elements, so the 16 threads of a
+// half-warp hit distinct 8-byte bank pairs in every access pattern used here, and a
+// round's 16 element offsets are linear in the register index (constant strides).
+__device__ __forceinline__ int pad(int f) { return f + (f >> 4); }
 
 __device__ __forceinline__ u64 tile_global(const PassParams& P, u64 tile, int f) {
   const int mid = P.q - P.c;  // bits between the low part and the target bits
@@ -158,13 +161,17 @@ __device__ __forceinline__ void apply_u(float2& x, float2& y, const float2 (&u)[
 }
 
 // One four-axis round: registers hold the 16 elements whose tile-local bits
-// [w0, w0+4) vary; axes in `mask` (tile-local) get the WHT (wht) or their unitary.
-__device__ void tile_round(float2* sm, const PassParams& P, int TB, int w0, unsigned mask, bool wht) {
+// [w0, w0+4) vary (w0 a multiple of 4); axes in `mask` (tile-local) get the WHT or
+// their unitary.  With the padded layout element i sits at pad(f0) + i * stride.
+__device__ void tile_round(float2* sm, const PassParams& P, int w0, unsigned mask, bool wht) {
   const int t = threadIdx.x;
   const int f0 = ((t >> w0) << (w0 + 4)) | (t & ((1 << w0) - 1));
+  const bool linear = (w0 & 3) == 0;  // windows clipped at a tile edge use general addressing
+  float2* base = sm + pad(f0);
+  const int stride = w0 >= 4 ? (1 << w0) + (1 << (w0 - 4)) : 1;
   float2 r[16];
 #pragma unroll
-  for (int i = 0; i < 16; ++i) r[i] = sm[swz(f0 | (i << w0))];
+  for (int i = 0; i < 16; ++i) r[i] = linear ? base[i * stride] : sm[pad(f0 | (i << w0))];
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     if (!((mask >> (w0 + a)) & 1u)) continue;
@@ -192,20 +199,23 @@ __device__ void tile_round(float2* sm, const PassParams& P, int TB, int w0, unsi
     }
   }
 #pragma unroll
-  for (int i = 0; i < 16; ++i) sm[swz(f0 | (i << w0))] = r[i];
-  (void)TB;
+  for (int i = 0; i < 16; ++i) {
+    if (linear)
+      base[i * stride] = r[i];
+    else
+      sm[pad(f0 | (i << w0))] = r[i];
+  }
 }
 
-// Four-axis rounds covering every axis of `mask`: each window starts at the lowest
-// axis not yet applied (clipped to the tile), so K target bits take ceil(K/4) rounds.
+// Rounds over the windows [0,4), [4,8), [8,12) that hold an axis of `mask`; in a tile
+// of TB < 12 bits the last window is clipped to [TB-4, TB) (its lower axes already done).
 __device__ void tile_rounds(float2* sm, const PassParams& P, int TB, unsigned mask, bool wht) {
-  while (mask) {
-    const int a = __ffs(mask) - 1;
-    const int w0 = a + 4 <= TB ? a : TB - 4;
-    const unsigned sel = mask & (15u << w0);
+  for (int g0 = 0; g0 < TB; g0 += 4) {
+    const int w0 = g0 + 4 <= TB ? g0 : TB - 4;
+    const unsigned sel = mask & (15u << w0) & ~((1u << g0) - 1u);
+    if (!sel) continue;
     __syncthreads();
-    tile_round(sm, P, TB, w0, sel, wht);
-    mask &= ~sel;
+    tile_round(sm, P, w0, sel, wht);
   }
   __syncthreads();
 }
@@ -226,8 +236,8 @@ __global__ void __launch_bounds__(256, 3) fourier_pass_kernel(const __grid_const
     for (int k = 0; k < 8; ++k) {
       const int f = 2 * (threadIdx.x + k * nt);
       const u64 g = tile_global(P, tile, f);
-      sm[swz(f)] = init_value(P, t, g);
-      sm[swz(f + 1)] = init_value(P, t, g + 1);
+      sm[pad(f)] = init_value(P, t, g);
+      sm[pad(f + 1)] = init_value(P, t, g + 1);
     }
   } else {
 #pragma unroll
@@ -241,8 +251,8 @@ __global__ void __launch_bounds__(256, 3) fourier_pass_kernel(const __grid_const
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const int f = 2 * (threadIdx.x + (h + k) * nt);
-        sm[swz(f)] = make_float2(x[k].x, x[k].y);
-        sm[swz(f + 1)] = make_float2(x[k].z, x[k].w);
+        sm[pad(f)] = make_float2(x[k].x, x[k].y);
+        sm[pad(f + 1)] = make_float2(x[k].z, x[k].w);
       }
     }
   }
@@ -259,8 +269,8 @@ __global__ void __launch_bounds__(256, 3) fourier_pass_kernel(const __grid_const
         u64 b, pm;
         tile_lut_eval(P.lut_a, t, g + e, b, pm);
         if (__popcll(pm) & 1) {
-          const float2 x = sm[swz(f + e)];
-          sm[swz(f + e)] = make_float2(-x.x, -x.y);
+          const float2 x = sm[pad(f + e)];
+          sm[pad(f + e)] = make_float2(-x.x, -x.y);
         }
       }
     }
@@ -271,9 +281,9 @@ __global__ void __launch_bounds__(256, 3) fourier_pass_kernel(const __grid_const
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const int f = 2 * (threadIdx.x + k * nt);
-    const float2 a = sm[swz(f)], b = sm[swz(f + 1)];
+    const float2 a = sm[pad(f)], b = sm[pad(f + 1)];
     if (P.store) *reinterpret_cast<float4*>(P.v + tile_global(P, tile, f)) = make_float4(a.x, a.y, b.x, b.y);
-    mass += (double)a.x * a.x + (double)a.y * a.y + (double)b.x * b.x + (double)b.y * b.y;
+    if (P.masses) mass += (double)a.x * a.x + (double)a.y * a.y + (double)b.x * b.x + (double)b.y * b.y;
   }
   if (P.masses) {
     __shared__ double red[32];
@@ -486,7 +496,7 @@ int set_smem_attr() {
   std::lock_guard<std::mutex> lock(g_fourier_mutex);
   if (device >= 0 && device < 64 && done[device]) return RGS_OK;
   RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (1 << kTileBits) * (int)sizeof(float2)));
+                                    ((1 << kTileBits) + (1 << (kTileBits - 4))) * (int)sizeof(float2)));
   if (device >= 0 && device < 64) done[device] = true;
   return RGS_OK;
 }
@@ -497,7 +507,7 @@ int launch_pass(const PassParams& P, cudaStream_t s) {
   const u64 tiles = 1ull << (P.m - TB);
   int rc = set_smem_attr();
   if (rc) return rc;
-  fourier_pass_kernel<<<(unsigned)tiles, 1 << (TB - 4), (1 << TB) * sizeof(float2), s>>>(P);
+  fourier_pass_kernel<<<(unsigned)tiles, 1 << (TB - 4), ((1 << TB) + (1 << (TB - 4))) * sizeof(float2), s>>>(P);
   RGS_CUDA_TRY(cudaGetLastError());
   return RGS_OK;
 }
