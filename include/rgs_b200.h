@@ -109,6 +109,30 @@ int rgs_scan_contract(rgs_plan* plan, const double* fvec, int64_t batch, int32_t
                       void* out_value, double* out_logscale, void* workspace, size_t workspace_bytes,
                       int32_t batch_tile, void* stream);
 
+/* ---------------------------------------------------------------- chain-rule sampler over the scan
+ * Exact Born sampling for any graph and order (no cut needed): the prefix marginal
+ * p(x_{v_0..v_{k-1}}) = 2^{-k} sum |E_k|^2 of the scan environment gives every
+ * conditional p(x_v | prefix) from one read of the table (both branches), and the
+ * chosen branch is then one scan step.  Extends the reference's p(x) path
+ * (W/upstream_scan/gpu_kernel.py:125-170) to sampling and conditional marginals;
+ * plans with fixed vertices are not supported.  batch_tile <= 128 (64 for C128).
+ * Workspace: rgs_chain_workspace_bytes().  check != 0 synchronises and reports a branch
+ * pair of zero total mass as RGS_ERR_ZERO_NORM. */
+int rgs_chain_workspace_bytes(const rgs_plan* plan, int32_t batch_tile, int32_t precision, size_t* bytes);
+/* count exact samples.  uniforms: device float64[count][n] in scan order, or NULL for
+ * Philox4x32-10 uniforms keyed by seed (counter = item, position).
+ * out_bits: device uint64[count][2]; out_value/out_logscale: the amplitude of each
+ * sample as rgs_scan_amplitudes; out_logp: device float64[count] = sum of log
+ * conditionals = log p(x) (may be NULL). */
+int rgs_chain_sample(rgs_plan* plan, const double* unitaries, int64_t count, uint64_t seed, const double* uniforms,
+                     int32_t precision, uint64_t* out_bits, void* out_value, double* out_logscale, double* out_logp,
+                     void* workspace, size_t workspace_bytes, int32_t batch_tile, int32_t check, void* stream);
+/* Conditional marginals of given bitstrings: out_cond1[i][j] = p(x_{v_j} = 1 | x_{v_0..v_{j-1}})
+ * (float32, scan order), out_logp[i] = log p(x_i), plus the amplitudes. */
+int rgs_chain_marginals(rgs_plan* plan, const double* unitaries, const uint64_t* bits, int64_t count,
+                        int32_t precision, float* out_cond1, double* out_logp, void* out_value, double* out_logscale,
+                        void* workspace, size_t workspace_bytes, int32_t batch_tile, int32_t check, void* stream);
+
 /* ---------------------------------------------------------------- conditional (Fourier-cut) sampler
  * Replaces DistributedSampler / FourierCovariantSampler / FusedFourierSampler /
  * DeferredGlobalMixin / SpecializedDeferredSampler (W/distributed_sampler.py:59-162,

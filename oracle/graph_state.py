@@ -289,3 +289,37 @@ def specialization_weight_table(unitary, outB, m):
             n00, n01, n10, n11 = m - r - k + h, k - h, r - h, h
             table[k, h] = 2.0 ** (-m / 2) * powers[0][n00] * powers[1][n01] * powers[2][n10] * powers[3][n11]
     return table
+
+
+# ----------------------------------------------------------------------------- chain-rule sampling
+def chain_conditionals(probs, order, bits):
+    """p(x_{v_j} = 1 | x_{v_0..v_{j-1}}) for every position j of a bitstring, from the full
+    probability vector (qubit q = index bit q).  Exact FP64 oracle for the scan chain rule."""
+    n = len(order)
+    idx = np.arange(len(probs), dtype=np.int64)
+    alive = np.ones(len(probs), dtype=bool)
+    out = np.zeros(n)
+    for j, v in enumerate(order):
+        tot = probs[alive].sum()
+        one = probs[alive & (((idx >> v) & 1) == 1)].sum()
+        out[j] = one / tot
+        alive &= ((idx >> v) & 1) == int(bits[v])
+    return out
+
+
+def chain_sample(probs, order, uniforms):
+    """Bitstring drawn position by position with x_v = 0 iff u * (M0 + M1) < M0, the
+    rule of the GPU chain sampler, given one uniform per position."""
+    n = len(order)
+    idx = np.arange(len(probs), dtype=np.int64)
+    alive = np.ones(len(probs), dtype=bool)
+    bits = np.zeros(n, dtype=np.uint8)
+    margins = np.zeros(n)
+    for j, v in enumerate(order):
+        m1 = probs[alive & (((idx >> v) & 1) == 1)].sum()
+        m0 = probs[alive].sum() - m1
+        x = 0 if uniforms[j] * (m0 + m1) < m0 else 1
+        margins[j] = abs(uniforms[j] * (m0 + m1) - m0) / (m0 + m1)
+        bits[v] = x
+        alive &= ((idx >> v) & 1) == x
+    return bits, margins

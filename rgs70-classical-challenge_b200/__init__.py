@@ -11,9 +11,10 @@ from .plan import ScanPlan, Step, make_plan, future_masks, rank_profile, byte_ta
 from .scan_oracle import ScanEngine, ScanOracle, pack_bits, amplitudes_from, PRECISIONS
 from . import instances
 from .samplers import ConditionalSampler, DrawRecorder, produce, fwht, product, block_mass
+from .chain import ChainSampler, unpack_bits
 
 __all__ = [
     "ScanPlan", "Step", "make_plan", "future_masks", "rank_profile", "byte_tables", "kernel_combos",
     "edges_from_graph", "ScanEngine", "ScanOracle", "pack_bits", "amplitudes_from", "PRECISIONS",
-    "ConditionalSampler", "DrawRecorder", "produce", "fwht", "product", "block_mass",
+    "ConditionalSampler", "DrawRecorder", "produce", "fwht", "product", "block_mass", "ChainSampler", "unpack_bits",
 ]

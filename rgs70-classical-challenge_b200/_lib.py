@@ -67,6 +67,13 @@ SIGNATURES = {
                                          c_void_p, c_void_p, ctypes.c_size_t, ctypes.c_int32, c_void_p]),
     "rgs_scan_amplitudes_noalloc": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_int64, ctypes.c_int32,
                                                    c_void_p, c_void_p, c_void_p]),
+    "rgs_chain_workspace_bytes": (ctypes.c_int, [c_void_p, ctypes.c_int32, ctypes.c_int32, c_size_t_p]),
+    "rgs_chain_sample": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int64, ctypes.c_uint64, c_void_p, ctypes.c_int32,
+                                        c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_size_t,
+                                        ctypes.c_int32, ctypes.c_int32, c_void_p]),
+    "rgs_chain_marginals": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_int64, ctypes.c_int32, c_void_p,
+                                           c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_size_t, ctypes.c_int32,
+                                           ctypes.c_int32, c_void_p]),
     "rgs_fourier_create": (ctypes.c_int, [ctypes.c_int32, c_uint8_p, c_double_p, ctypes.c_int32, c_int32_p,
                                           c_int32_p, ctypes.c_int32, ctypes.POINTER(c_void_p)]),
     "rgs_fourier_destroy": (None, [c_void_p]),

@@ -10,6 +10,7 @@
 #include "common.hpp"
 #include "plan.hpp"
 #include "scan.hpp"
+#include "chain.hpp"
 
 namespace rgs {
 
@@ -179,6 +180,33 @@ int rgs_scan_contract(rgs_plan* plan, const double* fvec, int64_t batch, int32_t
   if (!fvec) return fail(RGS_ERR_ARG, "fvec is required");
   return scan_run(plan->plan, nullptr, nullptr, fvec, batch, precision, out_value, out_logscale, workspace,
                   workspace_bytes, batch_tile, (cudaStream_t)stream, nullptr);
+}
+
+int rgs_chain_workspace_bytes(const rgs_plan* plan, int32_t batch_tile, int32_t precision, size_t* bytes) {
+  if (!plan || !bytes) return fail(RGS_ERR_ARG, "null argument");
+  ChainLayout L;
+  int rc = chain_layout(plan->plan, batch_tile, precision, L);
+  if (rc) return rc;
+  *bytes = L.total;
+  return RGS_OK;
+}
+
+int rgs_chain_sample(rgs_plan* plan, const double* unitaries, int64_t count, uint64_t seed, const double* uniforms,
+                     int32_t precision, uint64_t* out_bits, void* out_value, double* out_logscale, double* out_logp,
+                     void* workspace, size_t workspace_bytes, int32_t batch_tile, int32_t check, void* stream) {
+  if (!plan) return fail(RGS_ERR_ARG, "plan is NULL");
+  return chain_run(plan->plan, unitaries, count, 0, seed, uniforms, precision, (unsigned long long*)out_bits,
+                   out_value, out_logscale, out_logp, nullptr, workspace, workspace_bytes, batch_tile,
+                   (cudaStream_t)stream, check != 0);
+}
+
+int rgs_chain_marginals(rgs_plan* plan, const double* unitaries, const uint64_t* bits, int64_t count,
+                        int32_t precision, float* out_cond1, double* out_logp, void* out_value, double* out_logscale,
+                        void* workspace, size_t workspace_bytes, int32_t batch_tile, int32_t check, void* stream) {
+  if (!plan) return fail(RGS_ERR_ARG, "plan is NULL");
+  return chain_run(plan->plan, unitaries, count, 1, 0, nullptr, precision, (unsigned long long*)bits, out_value,
+                   out_logscale, out_logp, out_cond1, workspace, workspace_bytes, batch_tile, (cudaStream_t)stream,
+                   check != 0);
 }
 
 }  // extern "C"
