@@ -123,10 +123,12 @@ int rgs_chain_workspace_bytes(const rgs_plan* plan, int32_t batch_tile, int32_t 
  * Philox4x32-10 uniforms keyed by seed (counter = item, position).
  * out_bits: device uint64[count][2]; out_value/out_logscale: the amplitude of each
  * sample as rgs_scan_amplitudes; out_logp: device float64[count] = sum of log
- * conditionals = log p(x) (may be NULL). */
+ * conditionals = log p(x) (may be NULL); out_cond1: device float32[count][n], the
+ * conditionals p(x_{v_j} = 1 | prefix) met while sampling (may be NULL). */
 int rgs_chain_sample(rgs_plan* plan, const double* unitaries, int64_t count, uint64_t seed, const double* uniforms,
                      int32_t precision, uint64_t* out_bits, void* out_value, double* out_logscale, double* out_logp,
-                     void* workspace, size_t workspace_bytes, int32_t batch_tile, int32_t check, void* stream);
+                     float* out_cond1, void* workspace, size_t workspace_bytes, int32_t batch_tile, int32_t check,
+                     void* stream);
 /* Conditional marginals of given bitstrings: out_cond1[i][j] = p(x_{v_j} = 1 | x_{v_0..v_{j-1}})
  * (float32, scan order), out_logp[i] = log p(x_i), plus the amplitudes. */
 int rgs_chain_marginals(rgs_plan* plan, const double* unitaries, const uint64_t* bits, int64_t count,
@@ -187,6 +189,41 @@ int rgs_fwht(void* state, int32_t nbits, int32_t lo, int32_t hi, void* stream);
 int rgs_product(void* state, int32_t nbits, const double* unitaries, int32_t lo, int32_t hi, void* stream);
 /* masses[t] = sum |state|^2 over tile t of 2^tile_bits (blockmass, distributed_sampler.py:50-54). */
 int rgs_block_mass(const void* state, int32_t nbits, int32_t tile_bits, double* masses, void* stream);
+
+/* ---------------------------------------------------------------- learned proposal (MADE)
+ * No counterpart in the reference, which proposes uniformly (W/rejection_sampler.py:19);
+ * these are the kernels of the masked autoregressive proposal used for rejection
+ * sampling against the engine's p(x).  BF16 operands, FP32 accumulation on the tensor
+ * cores.  All pointers are device pointers; bf16 arrays are raw 16-bit values. */
+/* C[M][N] = alpha * op(A) op(B) (+ bias[N]) (relu) (* mask[M][N]) (* [gate[M][N] > 0]);
+ * A: [M][lda] (transA: [K][lda]); B: [K][ldb] (transB: [N][ldb]); C fp32 and/or Cb bf16. */
+int rgs_gemm_bf16(int32_t M, int32_t N, int32_t K, const void* A, int32_t lda, int32_t transA, const void* B,
+                  int32_t ldb, int32_t transB, float alpha, const float* bias, int32_t relu, const uint8_t* mask,
+                  const void* gate, float* C, void* Cb, int32_t ldc, void* stream);
+/* Forward: x bf16[batch][n] -> h1, h2 bf16[batch][hidden] -> logits z fp32[batch][n];
+ * weights bf16 W1[hidden][n], W2[hidden][hidden], W3[n][hidden] (already masked), biases fp32. */
+int rgs_mlp_fwd(int32_t batch, int32_t n, int32_t hidden, const void* x, const void* w1b, const float* b1,
+                const void* w2b, const float* b2, const void* w3b, const float* b3, void* h1b, void* h2b, float* z,
+                void* stream);
+/* Backward of the mean binary cross-entropy against soft targets (exact conditionals)
+ * target fp32[batch][n]: masked weight gradients gw* fp32, bias gradients gb*, scratch
+ * dz/dh2/dh1 bf16, and loss_blocks float64 partial sums of the (unscaled) loss. */
+int rgs_mlp_bwd(int32_t batch, int32_t n, int32_t hidden, const void* x, const void* w2b, const void* w3b,
+                const void* h1b, const void* h2b, const float* z, const float* target, const uint8_t* m1,
+                const uint8_t* m2, const uint8_t* m3, void* dzb, void* dh2b, void* dh1b, float* gw1, float* gb1,
+                float* gw2, float* gb2, float* gw3, float* gb3, double* loss_partials, int32_t loss_blocks,
+                void* stream);
+/* Adam step t (1-based) on fp32 masters w; refreshes the masked bf16 copy wb (may be NULL). */
+int rgs_mlp_adam(float* w, const float* grad, float* m1, float* m2, const uint8_t* mask, void* wb, int32_t count,
+                 float lr, float beta1, float beta2, float eps, int32_t t, void* stream);
+/* batch autoregressive samples x bf16[batch][n] and log q(x) (n forwards, hashed uniforms). */
+int rgs_mlp_sample(int32_t batch, int32_t n, int32_t hidden, const void* w1b, const float* b1, const void* w2b,
+                   const float* b2, const void* w3b, const float* b3, uint64_t seed, uint64_t first, void* x,
+                   double* logq, void* h1b, void* h2b, float* z, void* stream);
+/* log q(x) for given x bf16[batch][n]. */
+int rgs_mlp_logq(int32_t batch, int32_t n, int32_t hidden, const void* x, const void* w1b, const float* b1,
+                 const void* w2b, const float* b2, const void* w3b, const float* b3, double* logq, void* h1b,
+                 void* h2b, float* z, void* stream);
 
 /* ---------------------------------------------------------------- allocation-free scan
  * No counterpart in the reference.  Same result as rgs_scan_amplitudes, for callers

@@ -69,11 +69,23 @@ SIGNATURES = {
                                                    c_void_p, c_void_p, c_void_p]),
     "rgs_chain_workspace_bytes": (ctypes.c_int, [c_void_p, ctypes.c_int32, ctypes.c_int32, c_size_t_p]),
     "rgs_chain_sample": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int64, ctypes.c_uint64, c_void_p, ctypes.c_int32,
-                                        c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_size_t,
+                                        c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_size_t,
                                         ctypes.c_int32, ctypes.c_int32, c_void_p]),
     "rgs_chain_marginals": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_int64, ctypes.c_int32, c_void_p,
                                            c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_size_t, ctypes.c_int32,
                                            ctypes.c_int32, c_void_p]),
+    "rgs_gemm_bf16": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_void_p, ctypes.c_int32,
+                                     ctypes.c_int32, c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_float,
+                                     c_void_p, ctypes.c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
+                                     ctypes.c_int32, c_void_p]),
+    "rgs_mlp_fwd": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32] + [c_void_p] * 11),
+    "rgs_mlp_bwd": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32] + [c_void_p] * 20
+                    + [ctypes.c_int32, c_void_p]),
+    "rgs_mlp_adam": (ctypes.c_int, [c_void_p] * 6 + [ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                                      ctypes.c_float, ctypes.c_int32, c_void_p]),
+    "rgs_mlp_sample": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32] + [c_void_p] * 6
+                       + [ctypes.c_uint64, ctypes.c_uint64] + [c_void_p] * 6),
+    "rgs_mlp_logq": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32] + [c_void_p] * 12),
     "rgs_fourier_create": (ctypes.c_int, [ctypes.c_int32, c_uint8_p, c_double_p, ctypes.c_int32, c_int32_p,
                                           c_int32_p, ctypes.c_int32, ctypes.POINTER(c_void_p)]),
     "rgs_fourier_destroy": (None, [c_void_p]),

@@ -70,8 +70,9 @@ class ChainSampler:
                 torch.empty(count, dtype=torch.float64, device=self.device),
                 torch.empty(count, dtype=torch.float64, device=self.device))
 
-    def sample_device(self, count, seed=0, uniforms=None, check=True, stream=None, outs=None):
-        """Queue ``count`` samples; returns device tensors (bits, value, logscale, logp)."""
+    def sample_device(self, count, seed=0, uniforms=None, check=True, stream=None, outs=None, cond=None):
+        """Queue ``count`` samples; returns device tensors (bits, value, logscale, logp).
+        ``cond``: optional float32 [count, n] device tensor for the conditionals met."""
         bits = torch.empty((count, 2), dtype=torch.int64, device=self.device)
         value, logscale, logp = outs if outs is not None else self._outs(count)
         s = stream if stream is not None else torch.cuda.current_stream(self.device)
@@ -86,16 +87,20 @@ class ChainSampler:
                 self.plan.handle, ctypes.c_void_p(self.d_u.data_ptr()), count, int(seed) & (2 ** 64 - 1), uptr,
                 self.prec_code, ctypes.c_void_p(bits.data_ptr()), ctypes.c_void_p(value.data_ptr()),
                 ctypes.c_void_p(logscale.data_ptr()), ctypes.c_void_p(logp.data_ptr()),
+                ctypes.c_void_p(cond.data_ptr()) if cond is not None else None,
                 ctypes.c_void_p(self.workspace.data_ptr()), self.workspace.numel(), self.batch_tile,
                 1 if check else 0, ctypes.c_void_p(s.cuda_stream)))
         return bits, value, logscale, logp
 
-    def sample(self, count, seed=0, uniforms=None):
-        """(bits uint8 [count, n], p(x) float64 [count], log p(x) from the conditionals)."""
-        bits, value, logscale, logp = self.sample_device(count, seed, uniforms)
+    def sample(self, count, seed=0, uniforms=None, with_conditionals=False):
+        """(bits uint8 [count, n], p(x) float64 [count], log p(x) from the conditionals),
+        plus the conditionals p(x_{v_j} = 1 | prefix) [count, n] (scan order) if asked."""
+        cond = torch.empty((count, self.n), dtype=torch.float32, device=self.device) if with_conditionals else None
+        bits, value, logscale, logp = self.sample_device(count, seed, uniforms, cond=cond)
         b = unpack_bits(bits.cpu().numpy(), self.n)
         amp = amplitudes_from(value.cpu().numpy().astype(np.complex128), logscale.cpu().numpy(), self.n)
-        return b, np.abs(amp) ** 2, logp.cpu().numpy()
+        out = (b, np.abs(amp) ** 2, logp.cpu().numpy())
+        return out + (cond.cpu().numpy(),) if with_conditionals else out
 
     def marginals(self, bits):
         """Conditionals p(x_{v_j} = 1 | x_{v_<j}) [count, n] (scan order), log p(x), p(x)."""

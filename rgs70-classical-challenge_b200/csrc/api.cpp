@@ -193,10 +193,11 @@ int rgs_chain_workspace_bytes(const rgs_plan* plan, int32_t batch_tile, int32_t 
 
 int rgs_chain_sample(rgs_plan* plan, const double* unitaries, int64_t count, uint64_t seed, const double* uniforms,
                      int32_t precision, uint64_t* out_bits, void* out_value, double* out_logscale, double* out_logp,
-                     void* workspace, size_t workspace_bytes, int32_t batch_tile, int32_t check, void* stream) {
+                     float* out_cond1, void* workspace, size_t workspace_bytes, int32_t batch_tile, int32_t check,
+                     void* stream) {
   if (!plan) return fail(RGS_ERR_ARG, "plan is NULL");
   return chain_run(plan->plan, unitaries, count, 0, seed, uniforms, precision, (unsigned long long*)out_bits,
-                   out_value, out_logscale, out_logp, nullptr, workspace, workspace_bytes, batch_tile,
+                   out_value, out_logscale, out_logp, out_cond1, workspace, workspace_bytes, batch_tile,
                    (cudaStream_t)stream, check != 0);
 }
 

@@ -40,8 +40,10 @@ def test_given_uniforms_match_oracle(pkg, kind, n, seed, precision, tol):
         assert abs(logp[i] - np.log(probs[idx])) < (1e-4 if precision == "c64" else 1e-9)
         matched += 1
     assert matched > 0.95 * count
-    # Conditional marginals of the drawn strings.
+    # Conditional marginals of the drawn strings (teacher forcing), equal to those met while sampling.
     cond, lp, p2 = cs.marginals(bits)
+    _, _, _, cond_s = cs.sample(count, uniforms=uni, with_conditionals=True)
+    assert np.abs(cond - cond_s).max() < 1e-6
     for i in range(0, count, 17):
         ref = gs.chain_conditionals(probs, inst.order, bits[i])
         assert np.abs(cond[i] - ref).max() < max(tol, 2e-7)
