@@ -71,20 +71,24 @@ def trained(pkg):
     cond, _, _ = cs.marginals(bits)
     scan_bits = bits[:, inst.order]
     net = pkg.MadeProposal(inst.n, hidden=256, seed=1)
-    losses = net.fit(scan_bits, cond, epochs=6, batch=2048, lr=3e-3)
-    return inst, cs, net, losses
+    losses = net.fit(scan_bits, cond, epochs=12, batch=2048, lr=3e-3)
+    c = np.clip(cond.astype(np.float64), 1e-12, 1 - 1e-12)
+    floor = float(np.mean(np.sum(-(c * np.log(c) + (1 - c) * np.log(1 - c)), axis=1)))  # = H(p) by the chain rule
+    return inst, cs, net, (losses, floor)
 
 
 def test_training_learns_the_distribution(pkg, trained):
-    inst, cs, net, losses = trained
-    assert np.mean(losses[-5:]) < 0.8 * np.mean(losses[:5])
+    """Soft-target cross entropy has the floor H(p); training closes most of the gap."""
+    inst, cs, net, (losses, floor) = trained
+    assert np.mean(losses[-5:]) - floor < 0.5 * (np.mean(losses[:3]) - floor)
     probs = np.abs(gs.statevector(inst.g, inst.u)) ** 2
     allx = ((np.arange(1 << inst.n)[:, None] >> np.arange(inst.n)) & 1).astype(np.float32)
     lq = net.log_q(_bf(allx[:, inst.order])).cpu().numpy()
     q = np.exp(lq)
     assert abs(q.sum() - 1) < 1e-3                         # a normalised distribution
     kl = float(np.sum(probs * (np.log(probs) - lq)))
-    assert kl < 0.5 * float(np.sum(probs * (np.log(probs) + inst.n * np.log(2))))  # beats uniform by 2x
+    kl_uniform = float(np.sum(probs * (np.log(probs) + inst.n * np.log(2))))
+    assert kl < 0.5 * kl_uniform, (kl, kl_uniform)
 
 
 def test_proposal_samples_follow_q(pkg, trained):
