@@ -82,8 +82,15 @@ class MadeProposal:
         return [_p(w1), _p(b1), _p(w2), _p(b2), _p(w3), _p(b3)]
 
     # ------------------------------------------------------------------ device ops
+    def _input(self, x):
+        """Row-major bf16 [batch, n] on this device (the kernels read raw row-major memory)."""
+        if x.dim() != 2 or x.shape[1] != self.n:
+            raise ValueError(f"inputs must have shape (batch, {self.n})")
+        return x.to(device=self.device, dtype=torch.bfloat16).contiguous()
+
     def forward(self, x_bf16):
         """Logits z [batch, n] for bf16 inputs on the device."""
+        x_bf16 = self._input(x_bf16)
         batch = int(x_bf16.shape[0])
         buf = self._buffers(batch)
         with torch.cuda.device(self.device):
@@ -93,6 +100,10 @@ class MadeProposal:
 
     def gradients(self, x_bf16, target):
         """(loss, [gW1, gb1, gW2, gb2, gW3, gb3]) for one batch; target = exact conditionals."""
+        x_bf16 = self._input(x_bf16)
+        target = target.to(device=self.device, dtype=torch.float32).contiguous()
+        if tuple(target.shape) != tuple(x_bf16.shape):
+            raise ValueError("targets must match the inputs' shape")
         batch = int(x_bf16.shape[0])
         buf = self._buffers(batch)
         self.forward(x_bf16)
@@ -121,8 +132,8 @@ class MadeProposal:
 
     def fit(self, bits_scan, cond, epochs=4, batch=4096, lr=2e-3, seed=0):
         """Train on exact samples (bits in scan order) and their exact conditionals."""
-        x_all = torch.as_tensor(np.asarray(bits_scan, dtype=np.float32)).to(self.device).to(torch.bfloat16)
-        c_all = torch.as_tensor(np.asarray(cond, dtype=np.float32)).to(self.device)
+        x_all = torch.as_tensor(np.ascontiguousarray(bits_scan, dtype=np.float32)).to(self.device).to(torch.bfloat16)
+        c_all = torch.as_tensor(np.ascontiguousarray(cond, dtype=np.float32)).to(self.device)
         rng = np.random.default_rng(seed)
         losses = []
         count = len(x_all) - len(x_all) % batch
@@ -143,6 +154,7 @@ class MadeProposal:
         return buf["x"], buf["logq"]
 
     def log_q(self, x_bf16):
+        x_bf16 = self._input(x_bf16)
         batch = int(x_bf16.shape[0])
         buf = self._buffers(batch)
         with torch.cuda.device(self.device):

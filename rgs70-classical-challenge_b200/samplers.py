@@ -218,8 +218,18 @@ class ConditionalSampler:
 
 
 # ---------------------------------------------------------------------- building blocks
+def _state(state):
+    """The kernels address raw memory: the state must be a contiguous complex64 CUDA tensor."""
+    if state.dtype != torch.complex64 or not state.is_cuda or not state.is_contiguous() or state.dim() != 1:
+        raise ValueError("state must be a contiguous 1-D complex64 CUDA tensor")
+    if state.numel() & (state.numel() - 1):
+        raise ValueError("state length must be a power of two")
+    return state
+
+
 def fwht(state, lo=0, hi=None):
     """In-place Walsh-Hadamard butterflies on bits [lo, hi) of a complex64 CUDA tensor."""
+    _state(state)
     nbits = int(state.numel()).bit_length() - 1
     hi = nbits if hi is None else hi
     with torch.cuda.device(state.device):
@@ -228,6 +238,7 @@ def fwht(state, lo=0, hi=None):
 
 def product(state, unitaries, lo=0, hi=None):
     """In-place per-qubit 2x2 products (unitaries: complex [nbits, 2, 2]) on bits [lo, hi)."""
+    _state(state)
     nbits = int(state.numel()).bit_length() - 1
     hi = nbits if hi is None else hi
     u = torch.from_numpy(np.ascontiguousarray(np.asarray(unitaries, np.complex128)).view(np.float64).reshape(-1))
@@ -240,6 +251,7 @@ def product(state, unitaries, lo=0, hi=None):
 
 def block_mass(state, tile_bits):
     """Per-tile sum of |state|^2 (float64 CUDA tensor)."""
+    _state(state)
     nbits = int(state.numel()).bit_length() - 1
     out = torch.empty(1 << (nbits - tile_bits), dtype=torch.float64, device=state.device)
     with torch.cuda.device(state.device):

@@ -14,7 +14,17 @@ pytestmark = pytest.mark.gpu
 
 
 def _bf(a):
-    return torch.as_tensor(np.asarray(a, np.float32)).cuda().to(torch.bfloat16)
+    return torch.as_tensor(np.ascontiguousarray(a, np.float32)).cuda().to(torch.bfloat16)
+
+
+def test_inputs_of_any_layout(pkg):
+    """Column-permuted (non-contiguous) inputs give the same log q as their copies."""
+    net = pkg.MadeProposal(10, hidden=64, seed=2)
+    x = np.random.default_rng(0).integers(0, 2, (64, 10)).astype(np.float32)[:, ::-1]
+    t = torch.as_tensor(x)  # negative strides are copied by torch; transpose gives a non-contiguous view
+    a = net.log_q(t.T.contiguous().T.cuda()).cpu().numpy().copy()
+    b = net.log_q(torch.as_tensor(np.ascontiguousarray(x)).cuda()).cpu().numpy()
+    assert np.array_equal(a, b)
 
 
 @pytest.mark.parametrize("M,N,K,tA,tB", [(64, 64, 32, 0, 0), (100, 70, 45, 0, 1), (33, 130, 200, 1, 0),
