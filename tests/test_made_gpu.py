@@ -20,10 +20,11 @@ def _bf(a):
 def test_inputs_of_any_layout(pkg):
     """Column-permuted (non-contiguous) inputs give the same log q as their copies."""
     net = pkg.MadeProposal(10, hidden=64, seed=2)
-    x = np.random.default_rng(0).integers(0, 2, (64, 10)).astype(np.float32)[:, ::-1]
-    t = torch.as_tensor(x)  # negative strides are copied by torch; transpose gives a non-contiguous view
-    a = net.log_q(t.T.contiguous().T.cuda()).cpu().numpy().copy()
-    b = net.log_q(torch.as_tensor(np.ascontiguousarray(x)).cuda()).cpu().numpy()
+    x = np.random.default_rng(0).integers(0, 2, (64, 10)).astype(np.float32)
+    view = torch.as_tensor(np.ascontiguousarray(x.T)).cuda().T  # (64, 10), column-major view
+    assert not view.is_contiguous()
+    a = net.log_q(view).cpu().numpy().copy()
+    b = net.log_q(torch.as_tensor(x).cuda()).cpu().numpy()
     assert np.array_equal(a, b)
 
 
