@@ -82,7 +82,7 @@ def trained(pkg):
     cond, _, _ = cs.marginals(bits)
     scan_bits = bits[:, inst.order]
     net = pkg.MadeProposal(inst.n, hidden=256, seed=1)
-    losses = net.fit(scan_bits, cond, epochs=12, batch=2048, lr=3e-3)
+    losses = net.fit(scan_bits, cond, epochs=40, batch=1024, lr=5e-3)
     c = np.clip(cond.astype(np.float64), 1e-12, 1 - 1e-12)
     floor = float(np.mean(np.sum(-(c * np.log(c) + (1 - c) * np.log(1 - c)), axis=1)))  # = H(p) by the chain rule
     return inst, cs, net, (losses, floor)
