@@ -28,7 +28,7 @@ namespace rgs {
 
 namespace {
 
-constexpr int kMassBlocks = 592;  // 4 blocks on each of the 148 SMs of a B200
+constexpr int kMassBlocks = 296;  // 2 blocks (the occupancy of the mass kernel) on each of 148 SMs
 
 // Both branches of one position, reduced to per-item sums of |E'|^2 (double).  Layout
 // and geometry as scan_row_kernel; U_v rows (u0 = U_v[0,:], u1 = U_v[1,:]) are the same
@@ -221,17 +221,24 @@ __global__ void chain_decide_kernel(const double* __restrict__ partial, int nblo
                                     long long first, const double* __restrict__ uniforms, int n, u64 seed,
                                     double4* __restrict__ Wj, double* __restrict__ logp, float* __restrict__ cond1,
                                     int* __restrict__ status) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  // One warp per item: lanes sum strided block partials, then a fixed shuffle tree.
+  const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   if (b >= Bt) return;
   if (b >= count) {
-    Wj[b] = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (lane == 0) Wj[b] = make_double4(0.0, 0.0, 0.0, 0.0);
     return;
   }
   double m0 = 0.0, m1 = 0.0;
-  for (int k = 0; k < nblocks; ++k) {
+  for (int k = lane; k < nblocks; k += 32) {
     m0 += partial[((size_t)k * Bt + b) * 2 + 0];
     m1 += partial[((size_t)k * Bt + b) * 2 + 1];
   }
+  for (int off = 16; off; off >>= 1) {
+    m0 += __shfl_xor_sync(0xffffffffu, m0, off);
+    m1 += __shfl_xor_sync(0xffffffffu, m1, off);
+  }
+  if (lane) return;
   const double tot = m0 + m1;
   const long long item = first + b;
   int x;
@@ -359,7 +366,7 @@ int chain_run(Plan& plan, const double* U, long long count, int mode_given, u64 
       const int v = st.v;
       RGS_CUDA_TRY(launch_mass_step(precision, Bt, L.mass_blocks, stream, buf[j & 1], st, tables + st.table_off,
                                     U2 + (size_t)v * 4, j ? maxbuf + (size_t)(j - 1) * Bt : nullptr, partial, j == 0));
-      chain_decide_kernel<<<(Bt + 127) / 128, 128, 0, stream>>>(
+      chain_decide_kernel<<<(Bt * 32 + 127) / 128, 128, 0, stream>>>(
           partial, L.mass_blocks, Bt, cnt, j, v, U2, mode_given, bits, first, uniforms, plan.n, seed,
           W + (size_t)j * Bt, out_logp, out_cond1, status);
       RGS_CUDA_TRY(cudaGetLastError());
