@@ -135,6 +135,37 @@ int rgs_chain_marginals(rgs_plan* plan, const double* unitaries, const uint64_t*
                         int32_t precision, float* out_cond1, double* out_logp, void* out_value, double* out_logscale,
                         void* workspace, size_t workspace_bytes, int32_t batch_tile, int32_t check, void* stream);
 
+/* ---------------------------------------------------------------- resident batch of small instances
+ * Many (graph, gates, order) instances -- amplitudes of given bitstrings and exact
+ * chain-rule samples of each -- in ONE persistent launch: each block holds an
+ * instance's whole environment table for up to 64 items in shared memory and takes
+ * work units (largest first) from a device counter.  Replaces the per-instance loop
+ * over ScanOracle.amplitude / the scan sweep (W/scan_oracle.py:19-28,
+ * W/upstream_scan/gpu_kernel.py:125-170) for instances of rank <= rgs_batch_max_rank()
+ * (13 for complex64, 12 for complex128).  Amplitudes are bitwise equal to
+ * rgs_scan_amplitudes; samples use the Philox uniforms of rgs_chain_sample (same seed,
+ * same item -> same uniforms).  Plans with fixed vertices: amplitudes only.
+ * Every buffer of a batch lives on one device; a plan must outlive the batches that
+ * use it.  Adding instances is synchronous (it uploads the plan's tables once per
+ * device). */
+typedef struct rgs_batch rgs_batch;
+int rgs_batch_max_rank(int32_t precision, int32_t* rmax);
+int rgs_batch_create(int32_t precision, rgs_batch** out);
+void rgs_batch_destroy(rgs_batch* batch);
+/* One instance: count amplitudes of bits (device uint64[count][2]) into out_value /
+ * out_logscale (as rgs_scan_amplitudes), and nsamples samples with Philox key seed into
+ * sample_bits (uint64[nsamples][2]), sample_value / sample_logscale (their amplitudes)
+ * and sample_logp (log p(x) from the conditionals; may be NULL).  *index = its number. */
+int rgs_batch_add(rgs_batch* batch, rgs_plan* plan, const double* unitaries, const uint64_t* bits, int64_t count,
+                  void* out_value, double* out_logscale, int64_t nsamples, uint64_t seed, uint64_t* sample_bits,
+                  void* sample_value, double* sample_logscale, double* sample_logp, int32_t* index);
+int rgs_batch_info(const rgs_batch* batch, int32_t* instances, int64_t* units);
+/* Queues the whole batch on stream.  The first run after rgs_batch_add uploads the work
+ * list (synchronous); later runs are two stream operations (a counter reset and one
+ * kernel).  check != 0 synchronises and reports a zero-mass branch pair as
+ * RGS_ERR_ZERO_NORM. */
+int rgs_batch_run(rgs_batch* batch, int32_t check, void* stream);
+
 /* ---------------------------------------------------------------- conditional (Fourier-cut) sampler
  * Replaces DistributedSampler / FourierCovariantSampler / FusedFourierSampler /
  * DeferredGlobalMixin / SpecializedDeferredSampler (W/distributed_sampler.py:59-162,

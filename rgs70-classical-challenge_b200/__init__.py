@@ -12,12 +12,14 @@ from .scan_oracle import ScanEngine, ScanOracle, pack_bits, amplitudes_from, PRE
 from . import instances
 from .samplers import ConditionalSampler, DrawRecorder, produce, fwht, product, block_mass
 from .chain import ChainSampler, unpack_bits
+from .batch import ResidentBatch
+from . import batch
 from . import proposal
 from .proposal import MadeProposal, rejection_sample, capped_rejection, calibrate_envelope
 
 __all__ = [
     "ScanPlan", "Step", "make_plan", "future_masks", "rank_profile", "byte_tables", "kernel_combos",
     "edges_from_graph", "ScanEngine", "ScanOracle", "pack_bits", "amplitudes_from", "PRECISIONS",
-    "ConditionalSampler", "DrawRecorder", "produce", "fwht", "product", "block_mass", "ChainSampler", "unpack_bits",
+    "ConditionalSampler", "DrawRecorder", "produce", "fwht", "product", "block_mass", "ChainSampler", "unpack_bits", "ResidentBatch",
     "MadeProposal", "rejection_sample", "capped_rejection", "calibrate_envelope",
 ]

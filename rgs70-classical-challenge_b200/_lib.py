@@ -74,6 +74,14 @@ SIGNATURES = {
     "rgs_chain_marginals": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_int64, ctypes.c_int32, c_void_p,
                                            c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_size_t, ctypes.c_int32,
                                            ctypes.c_int32, c_void_p]),
+    "rgs_batch_max_rank": (ctypes.c_int, [ctypes.c_int32, c_int32_p]),
+    "rgs_batch_create": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(c_void_p)]),
+    "rgs_batch_destroy": (None, [c_void_p]),
+    "rgs_batch_add": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int64, c_void_p, c_void_p,
+                                     ctypes.c_int64, ctypes.c_uint64, c_void_p, c_void_p, c_void_p, c_void_p,
+                                     c_int32_p]),
+    "rgs_batch_info": (ctypes.c_int, [c_void_p, c_int32_p, ctypes.POINTER(ctypes.c_int64)]),
+    "rgs_batch_run": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_void_p]),
     "rgs_gemm_bf16": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_void_p, ctypes.c_int32,
                                      ctypes.c_int32, c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_float,
                                      c_void_p, ctypes.c_int32, c_void_p, c_void_p, c_void_p, c_void_p,

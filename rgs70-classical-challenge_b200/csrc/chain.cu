@@ -19,6 +19,7 @@
 
 #include "common.hpp"
 #include "chain.hpp"
+#include "philox.cuh"
 #include "plan.hpp"
 #include "scan.hpp"
 #include "scan_device.cuh"
@@ -188,28 +189,6 @@ __global__ void __launch_bounds__(256, 2) chain_mass_kernel(const S* __restrict_
     partial[((size_t)blockIdx.x * Bt + b) * 2 + 0] = s0;
     partial[((size_t)blockIdx.x * Bt + b) * 2 + 1] = s1;
   }
-}
-
-// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2,
-// 3", SC 2011): counter (item, position, stream, 0), key = seed.
-__device__ __forceinline__ uint4 philox4x32_10(uint4 ctr, uint2 key) {
-  const unsigned M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
-  for (int r = 0; r < 10; ++r) {
-    const unsigned hi0 = __umulhi(M0, ctr.x), lo0 = M0 * ctr.x;
-    const unsigned hi1 = __umulhi(M1, ctr.z), lo1 = M1 * ctr.z;
-    ctr = make_uint4(hi1 ^ ctr.y ^ key.x, lo1, hi0 ^ ctr.w ^ key.y, lo0);
-    key.x += W0;
-    key.y += W1;
-  }
-  return ctr;
-}
-
-// Uniform double in [0, 1) with 53 random bits.
-__device__ __forceinline__ double philox_uniform(u64 seed, u64 item, int position) {
-  const uint4 r = philox4x32_10(make_uint4((unsigned)item, (unsigned)(item >> 32), (unsigned)position, 0u),
-                                make_uint2((unsigned)seed, (unsigned)(seed >> 32)));
-  const u64 bits = (((u64)r.x << 32) | r.y) >> 11;
-  return (double)bits * 0x1.0p-53;
 }
 
 // Per item: M_x = sum over blocks of the partials (fixed order); x_v drawn with the

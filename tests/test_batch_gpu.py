@@ -1,0 +1,200 @@
+"""Resident batch executor (many small instances, one persistent launch) against the
+streaming executor, the chain-rule sampler and the FP64 statevector oracle.
+
+* Amplitudes are bitwise equal to the streaming executor's (same weights, fma order and
+  renormalisation), for every precision, uneven instance sizes and fixed vertices.
+* Samples equal the streaming chain sampler's for the same seed (the two sum branch
+  masses in different orders, so a decision whose uniform lies within rounding of a
+  branch boundary may differ: at most 1%), and follow the Born distribution.
+* A captured CUDA graph of the launch reproduces the results bit for bit.
+"""
+import numpy as np
+import pytest
+from scipy import stats
+
+from oracle import graph_state as gs
+
+pytestmark = pytest.mark.gpu
+
+
+def _instances(pkg, count, seed, nlo=12, nhi=26, rmax=None):
+    rng = np.random.default_rng(seed)
+    out = []
+    limit = rmax if rmax is not None else pkg.batch.max_rank("c128")
+    while len(out) < count:
+        n = int(rng.integers(nlo, nhi + 1))
+        kind = ["er3", "deg3", "reg3"][len(out) % 3]
+        if kind == "reg3" and n % 2:
+            n += 1
+        inst = pkg.instances.make_instance(kind, n, int(rng.integers(1 << 30)), pkg.rank_profile)
+        if inst.rmax <= limit:
+            out.append(inst)
+    return out
+
+
+@pytest.mark.parametrize("precision", ["c64", "c64f32", "c128"])
+def test_amplitudes_bitwise_equal_streaming(pkg, precision):
+    insts = _instances(pkg, 12, 1)
+    rng = np.random.default_rng(2)
+    rb = pkg.ResidentBatch(precision)
+    bits = []
+    for k, inst in enumerate(insts):
+        b = pkg.instances.uniform_bits([1, 7, 64, 130][k % 4], inst.n, rng)
+        bits.append(b)
+        rb.add(inst.g, inst.u, inst.order, bits=b)
+    rb.run()
+    for k, inst in enumerate(insts):
+        val, ls, amp = rb.amplitudes(k)
+        eng = pkg.ScanEngine(pkg.ScanPlan(inst.n, pkg.edges_from_graph(inst.g), inst.order), inst.u,
+                             precision=precision)
+        rv, rls = eng.sweep_bits(bits[k])
+        assert np.array_equal(val, rv) and np.array_equal(ls, rls), (k, inst.name)
+        if inst.n <= 20:
+            full = gs.statevector(inst.g, inst.u)
+            ref = full[(bits[k].astype(np.int64) << np.arange(inst.n)).sum(axis=1)]
+            rel = np.abs(np.abs(amp) ** 2 - np.abs(ref) ** 2) / np.abs(ref) ** 2
+            assert rel.max() < (1e-12 if precision == "c128" else 1e-4)
+
+
+def test_uneven_batch_and_largest_rank(pkg):
+    """Instances of rank 0 (edge-free) up to the resident maximum in one launch."""
+    rng = np.random.default_rng(5)
+    rmax = pkg.batch.max_rank("c64")
+    insts = _instances(pkg, 20, 6, nlo=4, nhi=30, rmax=rmax)
+    g0 = np.zeros((5, 5), dtype=np.uint8)
+    insts.append(pkg.instances.Instance(g0, pkg.instances.haar_su2(5, rng), list(range(5)), [0] * 5, "free5"))
+    g1 = np.zeros((1, 1), dtype=np.uint8)
+    insts.append(pkg.instances.Instance(g1, pkg.instances.haar_su2(1, rng), [0], [0], "single"))
+    # One instance at the largest rank that fits.
+    for s in range(200):
+        inst = pkg.instances.make_instance("er3", 34, 5000 + s, pkg.rank_profile, target_rank=rmax)
+        if inst.rmax == rmax:
+            insts.append(inst)
+            break
+    assert max(i.rmax for i in insts) == rmax
+    rb = pkg.ResidentBatch("c64")
+    bits = []
+    for inst in insts:
+        b = pkg.instances.uniform_bits(int(rng.integers(1, 100)), inst.n, rng)
+        bits.append(b)
+        rb.add(inst.g, inst.u, inst.order, bits=b)
+    rb.run()
+    for k, inst in enumerate(insts):
+        val, ls, _ = rb.amplitudes(k)
+        so = pkg.ScanOracle(inst.g, inst.u, inst.order)
+        rv, rls = so.engine.sweep_bits(bits[k])
+        assert np.array_equal(val, rv) and np.array_equal(ls, rls), inst.name
+
+
+def test_fixed_vertices(pkg):
+    rng = np.random.default_rng(21)
+    n = 14
+    g = pkg.instances.regular3(n, rng)
+    u = pkg.instances.haar_su2(n, rng)
+    for k, q in enumerate(rng.choice(n, size=5, replace=False)):
+        ph = np.exp(1j * rng.uniform(0, 2 * np.pi, 2))
+        u[q] = np.diag(ph) if k % 2 == 0 else np.array([[0, ph[0]], [ph[1], 0]])
+    from oracle import scan_plan as sp
+    fixed = sp.structurally_fixed(u, n)
+    order = rng.permutation(n).tolist()
+    plan = pkg.ScanPlan(n, pkg.edges_from_graph(g), order, fixed)
+    bits = pkg.instances.uniform_bits(200, n, rng)
+    for prec in ("c64", "c128"):
+        rb = pkg.ResidentBatch(prec)
+        rb.add(u=u, bits=bits, plan=plan)
+        rb.run()
+        val, ls, _ = rb.amplitudes(0)
+        rv, rls = pkg.ScanEngine(plan, u, precision=prec).sweep_bits(bits)
+        assert np.array_equal(val, rv) and np.array_equal(ls, rls)
+        with pytest.raises(NotImplementedError):
+            rb.add(u=u, nsamples=4, plan=plan)
+
+
+@pytest.mark.parametrize("precision", ["c64", "c128"])
+def test_samples_match_chain_sampler(pkg, precision):
+    insts = _instances(pkg, 6, 11, nlo=14, nhi=24)
+    rb = pkg.ResidentBatch(precision)
+    for k, inst in enumerate(insts):
+        rb.add(inst.g, inst.u, inst.order, nsamples=300, seed=100 + k)
+    rb.run()
+    total = diff = 0
+    for k, inst in enumerate(insts):
+        bits, p, logp = rb.samples(k)
+        cs = pkg.ChainSampler(inst.g, inst.u, inst.order, precision=precision)
+        rbits, rp, rlogp = cs.sample(300, seed=100 + k)
+        same = np.all(bits == rbits, axis=1)
+        total += len(same)
+        diff += int((~same).sum())
+        tol = 1e-12 if precision == "c128" else 1e-5
+        assert np.allclose(p[same], rp[same], rtol=tol, atol=0)
+        assert np.allclose(logp[same], rlogp[same], rtol=0, atol=1e-9 if precision == "c128" else 1e-5)
+        # log p from the conditionals equals log |amplitude|^2 of the drawn string.
+        assert np.abs(logp - np.log(p)).max() < (1e-9 if precision == "c128" else 1e-4)
+    assert diff <= 0.01 * total
+
+
+def test_born_distribution_and_mixed_work(pkg):
+    """Samples and amplitudes of the same instances in one launch."""
+    inst = pkg.instances.make_instance("reg3", 12, 7, pkg.rank_profile)
+    probs = np.abs(gs.statevector(inst.g, inst.u)) ** 2
+    rb = pkg.ResidentBatch("c64")
+    rng = np.random.default_rng(3)
+    bits_in = pkg.instances.uniform_bits(500, 12, rng)
+    for k in range(4):
+        rb.add(inst.g, inst.u, inst.order, bits=bits_in, nsamples=5000, seed=7000 + k)
+    rb.run()
+    idx = np.concatenate([(rb.samples(k)[0].astype(np.int64) << np.arange(12)).sum(axis=1) for k in range(4)])
+    G = 64
+    order = np.argsort(probs, kind="stable")
+    cm = np.cumsum(probs[order])
+    grp = np.empty(len(probs), np.int64)
+    grp[order] = np.minimum((cm * G).astype(np.int64), G - 1)
+    e = np.bincount(grp, weights=probs, minlength=G) * len(idx)
+    c = np.bincount(grp[idx], minlength=G)
+    assert stats.chi2.sf(((c - e) ** 2 / e).sum(), G - 1) > 1e-4
+    ref = probs[(bits_in.astype(np.int64) << np.arange(12)).sum(axis=1)]
+    for k in range(4):
+        _, _, amp = rb.amplitudes(k)
+        assert np.allclose(np.abs(amp) ** 2, ref, rtol=1e-4, atol=0)
+    # Different seeds draw different samples.
+    assert not np.array_equal(rb.samples(0)[0], rb.samples(1)[0])
+
+
+def test_graph_capture_replay(pkg):
+    insts = _instances(pkg, 8, 31)
+    rng = np.random.default_rng(31)
+    rb = pkg.ResidentBatch("c64")
+    for k, inst in enumerate(insts):
+        rb.add(inst.g, inst.u, inst.order, bits=pkg.instances.uniform_bits(50, inst.n, rng), nsamples=40, seed=k)
+    rb.run()
+    first = [(rb.amplitudes(k)[:2], rb.samples(k)) for k in range(len(insts))]
+    for e in rb.entries:
+        e.value.zero_()
+        e.sbits.zero_()
+    rb.capture()
+    rb.replay()
+    import torch
+    torch.cuda.synchronize()
+    for k in range(len(insts)):
+        (v0, l0), (b0, p0, lp0) = first[k]
+        v1, l1, _ = rb.amplitudes(k)
+        b1, p1, lp1 = rb.samples(k)
+        assert np.array_equal(v0, v1) and np.array_equal(l0, l1)
+        assert np.array_equal(b0, b1) and np.array_equal(lp0, lp1)
+
+
+def test_errors(pkg):
+    rb = pkg.ResidentBatch("c64")
+    big = None
+    for s in range(100):
+        inst = pkg.instances.make_instance("reg3", 40, 40 + s, pkg.rank_profile)
+        if inst.rmax > pkg.batch.max_rank("c64"):
+            big = inst
+            break
+    assert big is not None
+    with pytest.raises(NotImplementedError):
+        rb.add(big.g, big.u, big.order, bits=np.zeros((2, 40), dtype=np.uint8))
+    inst = pkg.instances.make_instance("reg3", 10, 1, pkg.rank_profile)
+    with pytest.raises(ValueError):
+        rb.add(inst.g, inst.u[:5], inst.order, bits=np.zeros((2, 10), dtype=np.uint8))
+    rb.run()  # an empty batch is a no-op
