@@ -616,6 +616,126 @@ def run_batched(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+# Published reference numbers for RGS70 (1x / 2x H200): 32 fixed inputs in 2.986 s (complex64,
+# frozen order) and 4.180 s (complex128); exact Born sampling 2.416 s per sample (2x H200).
+RGS70_REF_C64_AMP_PER_S = 32 / 2.986
+RGS70_REF_C128_AMP_PER_S = 32 / 4.180
+RGS70_REF_SAMPLES_PER_S_2GPU = 1 / 2.416
+
+
+def run_rgs70(args, rank, world, local_rank):
+    """The reference's own RGS70 instance (n = 70, 1150 edges, rank 30): p(x) of its 32
+    benchmark strings with the frozen order (complex64 and complex128), and exact Born
+    samples by the chain rule with the optimised order, each rescored in complex128."""
+    import torch
+    import torch.distributed as dist
+    from scipy import stats
+    import __graft_entry__
+    pkg = __graft_entry__.package()
+    device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+    if world > 1 and not dist.is_initialized():
+        dist.init_process_group("nccl", device_id=device)
+    fx = np.load(ROOT / "tests" / "golden" / "fixtures.npz")
+    rec = json.loads((ROOT / "tests" / "golden" / "rgs70_c128.json").read_text())
+    born = json.loads((ROOT / "tests" / "golden" / "rgs70_born.json").read_text())["probability_c128"]
+    g, u = fx["rgs70/graph"], fx["rgs70/measurement_unitaries"]
+    frozen, optimised = fx["rgs70/scan_order"].tolist(), fx["rgs70/scan_order_optimized"].tolist()
+    rows = rec["benchmark_rows"]
+    bits = np.array([[int(c) for c in r["bitstring_q0_left"]] for r in rows], dtype=np.uint8)
+    ref_p = np.array([r["probability_c128"] for r in rows])
+    stream = torch.cuda.current_stream(device)
+
+    def timed(fn, k):
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        return e0.elapsed_time(e1) / 1e3
+
+    def free():
+        torch.cuda.synchronize(device)
+        torch.cuda.empty_cache()
+
+    plan_f = pkg.ScanPlan(70, pkg.edges_from_graph(g), frozen)
+    plan_o = pkg.ScanPlan(70, pkg.edges_from_graph(g), optimised)
+    d_bits = torch.from_numpy(pkg.pack_bits(bits, 70).view(np.int64)).to(device)
+    legs = {}
+    with ClockSampler(local_rank) as clocks:
+        for prec, tile in (("c64", 8), ("c128", 4)):
+            eng = pkg.ScanEngine(plan_f, u, device=device, precision=prec, batch_tile=tile)
+            val, ls = eng.out_tensors(len(bits))
+            for _ in range(args.warmup if prec == "c64" else 1):
+                eng.run_bits(d_bits, val, ls, stream=stream)
+            t = timed(lambda: eng.run_bits(d_bits, val, ls, stream=stream), args.steps)
+            p = np.abs(pkg.amplitudes_from(val.cpu().numpy().astype(np.complex128), ls.cpu().numpy(), 70)) ** 2
+            esize = 16 if prec == "c128" else 8
+            legs[prec] = {"amplitudes_per_s": len(bits) * args.steps / t, "batch_tile": tile,
+                          "max_rel_err_vs_reference_c128": float(np.max(np.abs(p - ref_p) / ref_p)),
+                          "achieved_GBps": step_bytes(plan_f.ranks, esize) * len(bits) * args.steps / t / 1e9}
+            del eng, val, ls
+            free()
+        # Exact Born samples, optimised order, complex64 tables, 8 samples per tile.
+        S = 16
+        cs = pkg.ChainSampler(g, u, optimised, device=device, precision="c64", batch_tile=8)
+        outs = cs._outs(S)
+        seed = [70000 + 1000 * rank]
+
+        def sample():
+            seed[0] += 1
+            return cs.sample_device(S, seed=seed[0], check=False, stream=stream, outs=outs)
+        sample()
+        ts = timed(sample, args.steps)
+        sbits, sval, sls, slogp = sample()
+        torch.cuda.synchronize(device)
+        samples = pkg.unpack_bits(sbits.cpu().numpy(), 70)
+        p64 = np.abs(pkg.amplitudes_from(sval.cpu().numpy().astype(np.complex128), sls.cpu().numpy(), 70)) ** 2
+        lp = slogp.cpu().numpy()
+        del cs, outs, sbits, sval, sls, slogp
+        free()
+    so = pkg.ScanOracle(g, u, optimised, device=device, fp64=True, batch_tile=4)
+    p128 = so.probabilities(samples)
+    del so
+    free()
+    r_in = [0] + list(plan_o.ranks[:-1])
+    chain_bytes = 8 * sum((1 << a) * (j > 0) for j, a in enumerate(r_in)) + step_bytes(plan_o.ranks, 8)
+    z = p128 * 2.0 ** 70
+    zref = np.concatenate([born["batch1"], born["batch2"]]) * 2.0 ** 70
+    ks = stats.ks_2samp(z, zref)
+    rate_s = S * args.steps / ts
+    peaks_path = ROOT / "MEASURED_PEAKS.json"
+    peak = float(json.loads(peaks_path.read_text())["hbm_gbs"]) if peaks_path.exists() else 6650.0
+    value = legs["c64"]["amplitudes_per_s"]
+    line = {"metric": "amplitudes_per_s (p(x), RGS70 n=70 rank 30, frozen order, complex64)",
+            "value": world * value, "unit": "amplitudes/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * len(bits) / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": value / RGS70_REF_C64_AMP_PER_S, "dtype": "c64",
+            "data": "the reference's RGS70 instance and its 32 benchmark strings (fixtures from the reference)",
+            "config": {"workload": "RGS70 replay: n=70 dense (1150 edges), identical gates, frozen order r_max 30, "
+                                   "sum 2^r 9,982,443,517; 32 strings", "sum_states": plan_f.sum_states},
+            "roofline": {"bound": "hbm", "achieved": legs["c64"]["achieved_GBps"], "peak": peak, "unit": "GB/s",
+                         "frac": legs["c64"]["achieved_GBps"] / peak, "traffic": None},
+            "legs": legs,
+            "reference_published": {"c64_amplitudes_per_s_1xH200": RGS70_REF_C64_AMP_PER_S,
+                                    "c128_amplitudes_per_s_1xH200": RGS70_REF_C128_AMP_PER_S,
+                                    "born_samples_per_s_2xH200": RGS70_REF_SAMPLES_PER_S_2GPU},
+            "exact_born_samples": {
+                "value": rate_s, "unit": "samples/s", "order": "optimised (sum 2^r 7,919,632,381)",
+                "samples_per_step": S, "vs_reference_2xH200": rate_s / RGS70_REF_SAMPLES_PER_S_2GPU,
+                "achieved_GBps": chain_bytes * S * args.steps / ts / 1e9,
+                "max_rel_err_c64_vs_c128_rescore": float(np.max(np.abs(p64 - p128) / p128)),
+                "max_abs_logp_minus_log_p128": float(np.max(np.abs(lp - np.log(p128)))),
+                "linear_xeb_of_these_samples": float(z.mean() - 1),
+                "ks_vs_reference_born_samples": {"statistic": float(ks.statistic), "pvalue": float(ks.pvalue),
+                                                 "reference_samples": int(len(zref))}},
+            "gpu_launches": args.steps * -(-len(bits) // 8) * (70 + 2), "clocks": clocks.summary()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_learned(args, rank, world, local_rank):
     """Learned proposal workload: n=56 random degree<=3 graph (seeded order, max rank <= 28),
     MADE 2x512 trained on 2^16 exact samples + their exact conditionals; 4096 samples from
@@ -714,7 +834,7 @@ def main():
     ap.add_argument("--only", choices=["both", "c64", "c128"], default="both",
                     help="run only one precision (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
-    ap.add_argument("--workload", choices=["amplitudes", "fourier", "chain", "learned", "batched"], default="amplitudes")
+    ap.add_argument("--workload", choices=["amplitudes", "fourier", "chain", "learned", "batched", "rgs70"], default="amplitudes")
     ap.add_argument("--samples", type=int, default=4096, help="accepted samples of the learned workload")
     ap.add_argument("--epochs", type=int, default=8, help="training epochs of the learned workload")
     ap.add_argument("--m", type=int, default=30, help="conditional qubits of the fourier workload")
@@ -737,6 +857,8 @@ def main():
         run_learned(args, rank, world, local_rank)
     elif args.workload == "batched":
         run_batched(args, rank, world, local_rank)
+    elif args.workload == "rgs70":
+        run_rgs70(args, rank, world, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
 

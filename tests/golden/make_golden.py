@@ -15,9 +15,13 @@ input/output vectors that pin the CPU oracle (``oracle/``) and the CUDA engine:
                         deferred vectors and specialisation tables;
 * ``rgs70_c128.json``   a subset of the reference's stored complex128
                         probabilities for RGS70 bitstrings (the 32-input order
-                        benchmark rows and cap-1 scored records).
+                        benchmark rows and cap-1 scored records);
+* ``rgs70_born.json``   the complex128 probabilities of the reference's 3,452 exact
+                        Born samples of RGS70 (born/batch{1,2}/*_fp64.jsonl), the
+                        empirical law of p(x) under Born sampling.
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root:  python tests/golden/make_golden.py [born]
+(``born`` rewrites only rgs70_born.json).
 """
 import importlib.util
 import json
@@ -85,7 +89,28 @@ def plan_record(steps, ranks, fut):
     }
 
 
+def born_records():
+    """Complex128 scores of the reference's Born samples, in file order."""
+    born = REF / "born"
+    out = {}
+    for batch in ("batch1", "batch2"):
+        probs = []
+        for path in sorted((born / batch).glob("born*_group*_fp64.jsonl")):
+            for line in path.read_text().splitlines():
+                d = json.loads(line)
+                if "probability" in d and "bitstring_q0_left" in d:
+                    probs.append(d["probability"])
+        out[batch] = probs
+    (OUT / "rgs70_born.json").write_text(json.dumps({
+        "source": "reference born/batch{1,2}/born_group*_fp64.jsonl (complex128 rescoring of its exact Born samples)",
+        "n": 70, "probability_c128": out}))
+
+
 def main():
+    if sys.argv[1:] == ["born"]:
+        born_records()
+        return
+    born_records()
     sp = load("ref_scan_plan", W / "upstream_scan" / "scan_plan.py")
     sys.path.insert(0, str(W))
     gs = load("graph_sampler", W / "graph_sampler.py")

@@ -129,3 +129,18 @@ def test_gf2_maps_and_phases_bit_exact(fixtures, name):
         assert np.allclose(w, fixtures[f"{name}/spec_weights"], rtol=1e-14, atol=0)
         vals = w[gs.popcount64(b), gs.popcount64(b & np.uint64(sum(int(x) << j for j, x in enumerate(ob))))] * phase
         assert np.allclose(vals, fixtures[f"{name}/spec_values"], rtol=1e-13, atol=0)
+
+
+def test_rgs70_born_fixture_matches_published_xeb():
+    """The reference's Born-sample scores reproduce its published linear XEB
+    (born/README.md: 1.096 +- 0.035, 0.953 +- 0.033, pooled 1.025 +- 0.024)."""
+    import json
+    from conftest import GOLDEN
+    d = json.loads((GOLDEN / "rgs70_born.json").read_text())["probability_c128"]
+    z1 = np.array(d["batch1"]) * 2.0 ** 70
+    z2 = np.array(d["batch2"]) * 2.0 ** 70
+    assert len(z1) == len(z2) == 1726
+    assert abs(z1.mean() - 1 - 1.096) < 5e-4 and abs(z1.std(ddof=1) / np.sqrt(1726) - 0.035) < 5e-4
+    assert abs(z2.mean() - 1 - 0.953) < 5e-4 and abs(z2.std(ddof=1) / np.sqrt(1726) - 0.033) < 5e-4
+    zz = np.concatenate([z1, z2])
+    assert abs(zz.mean() - 1 - 1.025) < 5e-4 and abs(zz.std(ddof=1) / np.sqrt(len(zz)) - 0.024) < 5e-4
