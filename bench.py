@@ -48,6 +48,14 @@ def step_bytes(ranks, esize):
     return esize * sum((1 << a) * (j > 0) + (1 << b) for j, (a, b) in enumerate(zip(r_in, ranks)))
 
 
+def chain_bytes(plan, esize):
+    """Compulsory table traffic of one chain-rule sample: the scan sweep, plus one read of
+    the input table of every position whose branch masses need the Gram pass (a
+    position with an empty kernel has them in closed form)."""
+    gram = sum((1 << st.r_in) for j, st in enumerate(plan.steps) if j > 0 and len(st.kernel) > 0)
+    return step_bytes(plan.ranks, esize) + esize * gram
+
+
 def reference_bytes(ranks, esize):
     """Byte model of the reference kernel: every input read twice (each output gathers
     its pre-images), every output written once."""
@@ -286,8 +294,15 @@ def run_ours(args, rank, world, local_rank):
     if peaks_path.exists():
         peak, peak_src = float(json.loads(peaks_path.read_text())["hbm_gbs"]), "measured"
     achieved = (b64 + b128) / (t_step / args.steps) / 1e9
+    # DRAM traffic of one tile sweep from one ncu capture, times the tiles of this step
+    # (valid for the tile sizes it was captured at).
+    traffic = None
     traffic_path = ROOT / "profiles" / "scan_step_traffic.json"
-    traffic = json.loads(traffic_path.read_text()).get("dram_bytes_per_step") if traffic_path.exists() else None
+    if traffic_path.exists():
+        tr = json.loads(traffic_path.read_text())["dram_bytes_per_tile"]
+        if (not use64 or tr["c64"]["tile"] == tile64) and (not use128 or tr["c128"]["tile"] == tile128):
+            traffic = ((math.ceil(BATCH / tile64) * tr["c64"]["bytes"] if use64 else 0)
+                       + (math.ceil(BATCH / tile128) * tr["c128"]["bytes"] if use128 else 0))
     groups64 = math.ceil(BATCH / tile64) if use64 else 0
     groups128 = math.ceil(BATCH / tile128) if use128 else 0
     launches = args.steps * ((groups64 + groups128) * (N_QUBITS + 2))
@@ -459,10 +474,8 @@ def run_chain(args, rank, world, local_rank, emit=True):
     lp = logp.cpu().numpy()
     consistency = float(np.max(np.abs(np.log(p) - lp)))
     xeb = float((2.0 ** N_QUBITS) * p.mean() - 1)
-    # Table traffic per sample: the branch-mass pass reads each table once, the step reads
-    # and writes it (compulsory bytes).
-    r_in = [0] + list(inst.ranks[:-1])
-    bytes_per = 8 * sum((1 << a) * (j > 0) for j, a in enumerate(r_in)) + step_bytes(inst.ranks, 8)
+    # Table traffic per sample (compulsory bytes): the sweep, plus the Gram reads.
+    bytes_per = chain_bytes(cs.plan, 8)
     line = {"metric": "exact_born_samples_per_s (chain rule over the scan, n=40 3-regular)",
             "value": world * BATCH * args.steps / t, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -589,10 +602,8 @@ def run_batched(args, rank, world, local_rank):
     # Table traffic in shared memory per step (the streaming executor's compulsory HBM bytes
     # for the same sweeps; samples also read every table once for the branch masses).
     tb = 0
-    for inst in insts:
-        r_in = [0] + list(inst.ranks[:-1])
-        mass = 8 * sum((1 << a) * (j > 0) for j, a in enumerate(r_in))
-        tb += K * step_bytes(inst.ranks, 8) + S * (step_bytes(inst.ranks, 8) + mass)
+    for inst, plan in zip(insts, plans):
+        tb += K * step_bytes(inst.ranks, 8) + S * chain_bytes(plan, 8)
     smem_peak = 148 * 128 * 1.965e9 / 1e9  # nominal: 128 B/clock/SM at the maximum SM clock
     line = {"metric": "batched_items_per_s (amplitudes + exact samples, 1024 uneven instances, one launch)",
             "value": world * items * args.steps / t, "unit": "items/s", "n_gpus": world, "steps": args.steps,
@@ -700,8 +711,7 @@ def run_rgs70(args, rank, world, local_rank):
     p128 = so.probabilities(samples)
     del so
     free()
-    r_in = [0] + list(plan_o.ranks[:-1])
-    chain_bytes = 8 * sum((1 << a) * (j > 0) for j, a in enumerate(r_in)) + step_bytes(plan_o.ranks, 8)
+    sample_bytes = chain_bytes(plan_o, 8)
     z = p128 * 2.0 ** 70
     zref = np.concatenate([born["batch1"], born["batch2"]]) * 2.0 ** 70
     ks = stats.ks_2samp(z, zref)
@@ -725,7 +735,7 @@ def run_rgs70(args, rank, world, local_rank):
             "exact_born_samples": {
                 "value": rate_s, "unit": "samples/s", "order": "optimised (sum 2^r 7,919,632,381)",
                 "samples_per_step": S, "vs_reference_2xH200": rate_s / RGS70_REF_SAMPLES_PER_S_2GPU,
-                "achieved_GBps": chain_bytes * S * args.steps / ts / 1e9,
+                "achieved_GBps": sample_bytes * S * args.steps / ts / 1e9,
                 "max_rel_err_c64_vs_c128_rescore": float(np.max(np.abs(p64 - p128) / p128)),
                 "max_abs_logp_minus_log_p128": float(np.max(np.abs(lp - np.log(p128)))),
                 "linear_xeb_of_these_samples": float(z.mean() - 1),

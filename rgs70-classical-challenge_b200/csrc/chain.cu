@@ -6,12 +6,15 @@
 // (trace out the unmeasured suffix: unitarity of each U_q, then Parseval over the
 // syndrome subspace).  So p(x_v = x | prefix) = M_x / (M_0 + M_1) with M_x the squared
 // norm of the table after position v with branch x.  Per position this file runs
-//   chain_mass_kernel   : both branches' sum |E'|^2 per item from one read of E (no writes)
+//   chain_gram_kernel   : a 2x2 Gram matrix per item from one read of E (no writes), from
+//                         which both branch masses follow; skipped on positions whose
+//                         step pairs each input row with two output rows through one
+//                         combo, where M_0 and M_1 are known in closed form
 //   chain_decide_kernel : per item, exact inverse-CDF choice of x_v (or the given bit),
 //                         log p(x_v | prefix), and the weights of the chosen branch
 //   scan step kernel    : the chosen branch, with the usual power-of-two renormalisation
-// so a sample costs one read of every table plus one scan sweep.  The final table is the
-// amplitude of the drawn string, returned like rgs_scan_amplitudes.
+// so a sample costs one scan sweep plus one read of the tables of the other positions.
+// The final table is the amplitude of the drawn string, returned like rgs_scan_amplitudes.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -29,19 +32,24 @@ namespace rgs {
 
 namespace {
 
-constexpr int kMassBlocks = 296;  // 2 blocks (the occupancy of the mass kernel) on each of 148 SMs
+constexpr int kMassBlocks = 296;   // 2 blocks (the occupancy of the Gram kernel) on each of 148 SMs
+constexpr int kChainMaxTile = 128;  // largest batch tile (complex64); complex128: 64
 
-// Both branches of one position, reduced to per-item sums of |E'|^2 (double).  Layout
-// and geometry as scan_row_kernel; U_v rows (u0 = U_v[0,:], u1 = U_v[1,:]) are the same
-// for every item, the scale 2^-e is per item.
-template <typename S, typename M, int VE, int MODE, int NC, int CPL>
-__global__ void __launch_bounds__(256, 2) chain_mass_kernel(const S* __restrict__ Ein, const __grid_constant__ DevStep st,
-                                                            const u64* __restrict__ T, const double2* __restrict__ Uv,
-                                                            const u64* __restrict__ maxprev,
-                                                            double* __restrict__ partial, int lbt, int unit_input) {
-  constexpr int U = RowsPerIter<NC, CPL, LoadsInFlight<S, M>::value>::value;
+// Gram matrix of one position per item, from one read of the table (no writes).  Every
+// output of the step is alpha f(0) + beta f(1) with f = U_v[x, :] s: in pair mode row c'
+// has alpha = sum_{y=0} e, beta = sum_{y=1} (-1)^par e, and row c'^t the mirror image
+// (alpha = sum_{y=1} e, beta = sum_{y=0} (-1)^par e); in merge mode alpha = sum e,
+// beta = sum (-1)^par e.  Both branch masses then follow from
+//   G = sum over outputs of ( |alpha|^2, |beta|^2, alpha conj(beta) ):
+//   M_x / s^2 = G00 |U_x0|^2 + G11 |U_x1|^2 + 2 Re(G01 U_x0 conj(U_x1)),
+// one accumulation for the two branches.  Layout and geometry as scan_row_kernel.
+template <typename S, int VE, int MODE, int NC, int CPL>
+__global__ void __launch_bounds__(256, 2) chain_gram_kernel(const S* __restrict__ Ein, const __grid_constant__ DevStep st,
+                                                            const u64* __restrict__ T, double* __restrict__ partial,
+                                                            int lbt, int unit_input) {
+  constexpr int U = RowsPerIter<NC, CPL, LoadsInFlight<S, double>::value>::value;
   constexpr int NI = CPL * VE;
-  __shared__ double red[8][256][2];  // per warp, per item, per branch
+  __shared__ double red[8][kChainMaxTile][4];  // per warp, per item: G00, G11, Re G01, Im G01
   const int Bt = 1 << lbt;
   const int lC = lbt - (VE == 2 ? 1 : 0);
   const int lL = lC < 5 ? lC : 5;
@@ -50,36 +58,14 @@ __global__ void __launch_bounds__(256, 2) chain_mass_kernel(const S* __restrict_
   const int sub = lane >> lL;
   const int l = lane & ((1 << lL) - 1);
 
-  // Branch weights (scaled per item): x = 0 uses (a0, a1) = u0, x = 1 uses u1.
-  Cx<M> w[2][NI][2];
-  for (int k = 0; k < CPL; ++k)
-    for (int v = 0; v < VE; ++v) {
-      const int i = k * VE + v, b = ((l + (k << lL)) * VE) + v;
-      const double m2 = maxprev ? max_value<S>(maxprev[b]) : 1.0;
-      const double s = ldexp(1.0, -scale_exponent(m2));
-      const double4 uu[2] = {make_double4(Uv[0].x, Uv[0].y, Uv[1].x, Uv[1].y),
-                             make_double4(Uv[2].x, Uv[2].y, Uv[3].x, Uv[3].y)};
-      for (int x = 0; x < 2; ++x) {
-        double ar = uu[x].x * s, ai = uu[x].y * s, br = uu[x].z * s, bi = uu[x].w * s;
-        if (MODE == MODE_MERGE) {
-          const double pr = ar + br, pim = ai + bi, mr = ar - br, mi = ai - bi;
-          ar = pr;
-          ai = pim;
-          br = mr;
-          bi = mi;
-        }
-        w[x][i][0] = Cx<M>{(M)ar, (M)ai};
-        w[x][i][1] = Cx<M>{(M)br, (M)bi};
-      }
-    }
-
   const u64 items = (MODE == MODE_PAIR) ? (1ull << (st.r_out - 1)) : (1ull << st.r_out);
   const u64 warp = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
   const u64 per_iter = (u64)U << lR;
   const u64 mask = (1ull << st.r_in) - 1ull;
-  double acc[NI][2];
-  for (int i = 0; i < NI; ++i) acc[i][0] = acc[i][1] = 0.0;
+  double g[NI][4];
+#pragma unroll
+  for (int i = 0; i < NI; ++i) g[i][0] = g[i][1] = g[i][2] = g[i][3] = 0.0;
 
   for (u64 base = warp * per_iter; base < items; base += nwarps * per_iter) {
     u64 cc[U][NC];
@@ -119,38 +105,40 @@ __global__ void __launch_bounds__(256, 2) chain_mass_kernel(const S* __restrict_
 #pragma unroll
         for (int v = 0; v < VE; ++v) {
           const int i = j * VE + v;
+          double aar = 0.0, aai = 0.0, bar = 0.0, bai = 0.0;  // alpha, beta of row c'
+          double car = 0.0, cai = 0.0, dbr = 0.0, dbi = 0.0;  // alpha, beta of row c'^t (pair mode)
 #pragma unroll
-          for (int x = 0; x < 2; ++x) {
-            Cx<M> oa{(M)0, (M)0}, ob{(M)0, (M)0};
-#pragma unroll
-            for (int k = 0; k < NC; ++k) {
-              const M er = (M)e[u][k][j].re(v), ei = (M)e[u][k][j].im(v);
-              const int par = pc[u][k];
-              if (MODE == MODE_PAIR) {
-                const int y = yy[u][k];
-                Cx<M> wa = y ? w[x][i][1] : w[x][i][0];
-                Cx<M> wb = y ? w[x][i][0] : w[x][i][1];
-                if (y & par) {
-                  wa.re = -wa.re;
-                  wa.im = -wa.im;
-                }
-                if ((y ^ 1) & par) {
-                  wb.re = -wb.re;
-                  wb.im = -wb.im;
-                }
-                cmad(oa, er, ei, wa);
-                cmad(ob, er, ei, wb);
-              } else {
-                cmad(oa, er, ei, par ? w[x][i][1] : w[x][i][0]);
-              }
-            }
-            // Squared moduli of the values the step kernel would store (rounded to S).
-            const S ar = (S)oa.re, ai = (S)oa.im;
-            acc[i][x] += (double)norm2(ar, ai);
+          for (int k = 0; k < NC; ++k) {
+            const double er = (double)e[u][k][j].re(v), ei = (double)e[u][k][j].im(v);
+            const double sr = pc[u][k] ? -er : er, si = pc[u][k] ? -ei : ei;
             if (MODE == MODE_PAIR) {
-              const S br = (S)ob.re, bi = (S)ob.im;
-              acc[i][x] += (double)norm2(br, bi);
+              if (yy[u][k]) {
+                car += er;
+                cai += ei;
+                bar += sr;
+                bai += si;
+              } else {
+                aar += er;
+                aai += ei;
+                dbr += sr;
+                dbi += si;
+              }
+            } else {
+              aar += er;
+              aai += ei;
+              bar += sr;
+              bai += si;
             }
+          }
+          g[i][0] = fma(aar, aar, fma(aai, aai, g[i][0]));
+          g[i][1] = fma(bar, bar, fma(bai, bai, g[i][1]));
+          g[i][2] = fma(aar, bar, fma(aai, bai, g[i][2]));
+          g[i][3] = fma(aai, bar, fma(-aar, bai, g[i][3]));
+          if (MODE == MODE_PAIR) {
+            g[i][0] = fma(car, car, fma(cai, cai, g[i][0]));
+            g[i][1] = fma(dbr, dbr, fma(dbi, dbi, g[i][1]));
+            g[i][2] = fma(car, dbr, fma(cai, dbi, g[i][2]));
+            g[i][3] = fma(cai, dbr, fma(-car, dbi, g[i][3]));
           }
         }
     }
@@ -161,13 +149,13 @@ __global__ void __launch_bounds__(256, 2) chain_mass_kernel(const S* __restrict_
 #pragma unroll
   for (int i = 0; i < NI; ++i)
 #pragma unroll
-    for (int x = 0; x < 2; ++x) {
-      double a = acc[i][x];
+    for (int q = 0; q < 4; ++q) {
+      double a = g[i][q];
       for (int off = 16; off >= (1 << lL); off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
-      acc[i][x] = a;
+      g[i][q] = a;
     }
   for (int b = threadIdx.x; b < Bt; b += blockDim.x)
-    for (int wv = 0; wv < 8; ++wv) red[wv][b][0] = red[wv][b][1] = 0.0;
+    for (int wv = 0; wv < 8; ++wv) red[wv][b][0] = red[wv][b][1] = red[wv][b][2] = red[wv][b][3] = 0.0;
   __syncthreads();
   if (sub == 0) {
 #pragma unroll
@@ -175,28 +163,36 @@ __global__ void __launch_bounds__(256, 2) chain_mass_kernel(const S* __restrict_
 #pragma unroll
       for (int v = 0; v < VE; ++v) {
         const int i = k * VE + v, b = ((l + (k << lL)) * VE) + v;
-        red[wib][b][0] = acc[i][0];
-        red[wib][b][1] = acc[i][1];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) red[wib][b][q] = g[i][q];
       }
   }
   __syncthreads();
   for (int b = threadIdx.x; b < Bt; b += blockDim.x) {
-    double s0 = 0.0, s1 = 0.0;
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
     for (int wv = 0; wv < (int)(blockDim.x >> 5); ++wv) {
-      s0 += red[wv][b][0];
-      s1 += red[wv][b][1];
+      t0 += red[wv][b][0];
+      t1 += red[wv][b][1];
+      t2 += red[wv][b][2];
+      t3 += red[wv][b][3];
     }
-    partial[((size_t)blockIdx.x * Bt + b) * 2 + 0] = s0;
-    partial[((size_t)blockIdx.x * Bt + b) * 2 + 1] = s1;
+    double* p = partial + ((size_t)blockIdx.x * Bt + b) * 4;
+    p[0] = t0;
+    p[1] = t1;
+    p[2] = t2;
+    p[3] = t3;
   }
 }
 
-// Per item: M_x = sum over blocks of the partials (fixed order); x_v drawn with the
-// item's uniform (x = 0 iff u (M0 + M1) < M0) or taken from the given bits; then the
-// chosen branch's weights for the step kernel, the sampled bit, log p(x_v | prefix) and
-// the conditional probability p(x_v = 1 | prefix).
-__global__ void chain_decide_kernel(const double* __restrict__ partial, int nblocks, int Bt, int count, int j, int v,
-                                    const double2* __restrict__ U, int mode_given, u64* __restrict__ bits,
+// Per item: the Gram matrix (sum over blocks of the partials, fixed order; or, on a
+// position whose step pairs every input row with two output rows through one combo,
+// G = identity: there M_x = sum|E|^2 s^2 (|U_x0|^2 + |U_x1|^2) for both x -- the new
+// syndrome bit is uniform, and no pass over the table is needed); the branch masses M_x;
+// x_v drawn with the item's uniform (x = 0 iff u (M0 + M1) < M0) or taken from the given
+// bits; then the chosen branch's weights for the step kernel, the sampled bit,
+// log p(x_v | prefix) and the conditional probability p(x_v = 1 | prefix).
+__global__ void chain_decide_kernel(const double* __restrict__ partial, int nblocks, int analytic, int Bt, int count,
+                                    int j, int v, const double2* __restrict__ U, int mode_given, u64* __restrict__ bits,
                                     long long first, const double* __restrict__ uniforms, int n, u64 seed,
                                     double4* __restrict__ Wj, double* __restrict__ logp, float* __restrict__ cond1,
                                     int* __restrict__ status) {
@@ -208,16 +204,26 @@ __global__ void chain_decide_kernel(const double* __restrict__ partial, int nblo
     if (lane == 0) Wj[b] = make_double4(0.0, 0.0, 0.0, 0.0);
     return;
   }
-  double m0 = 0.0, m1 = 0.0;
-  for (int k = lane; k < nblocks; k += 32) {
-    m0 += partial[((size_t)k * Bt + b) * 2 + 0];
-    m1 += partial[((size_t)k * Bt + b) * 2 + 1];
-  }
-  for (int off = 16; off; off >>= 1) {
-    m0 += __shfl_xor_sync(0xffffffffu, m0, off);
-    m1 += __shfl_xor_sync(0xffffffffu, m1, off);
+  double g0 = 1.0, g1 = 1.0, g2 = 0.0, g3 = 0.0;
+  if (!analytic) {
+    g0 = g1 = 0.0;
+    for (int k = lane; k < nblocks; k += 32) {
+      const double* p = partial + ((size_t)k * Bt + b) * 4;
+      g0 += p[0];
+      g1 += p[1];
+      g2 += p[2];
+      g3 += p[3];
+    }
+    for (int off = 16; off; off >>= 1) {
+      g0 += __shfl_xor_sync(0xffffffffu, g0, off);
+      g1 += __shfl_xor_sync(0xffffffffu, g1, off);
+      g2 += __shfl_xor_sync(0xffffffffu, g2, off);
+      g3 += __shfl_xor_sync(0xffffffffu, g3, off);
+    }
   }
   if (lane) return;
+  const double m0 = branch_mass(U + (v * 2 + 0) * 2, g0, g1, g2, g3);
+  const double m1 = branch_mass(U + (v * 2 + 1) * 2, g0, g1, g2, g3);
   const double tot = m0 + m1;
   const long long item = first + b;
   int x;
@@ -252,51 +258,44 @@ __global__ void chain_zero_kernel(double* x, long long first, int count) {
 }
 
 // ------------------------------------------------------------------------------- host
-template <typename S, typename M, int VE, int CPL, int MODE, int NC>
-cudaError_t launch_mass(dim3 grid, cudaStream_t s, const void* Ein, const DevStep& st, const u64* T,
-                        const double2* Uv, const u64* mp, double* partial, int lbt, int unit) {
-  chain_mass_kernel<S, M, VE, MODE, NC, CPL><<<grid, 256, 0, s>>>((const S*)Ein, st, T, Uv, mp, partial, lbt, unit);
+template <typename S, int VE, int CPL, int MODE, int NC>
+cudaError_t launch_gram(dim3 grid, cudaStream_t s, const void* Ein, const DevStep& st, const u64* T, double* partial,
+                        int lbt, int unit) {
+  chain_gram_kernel<S, VE, MODE, NC, CPL><<<grid, 256, 0, s>>>((const S*)Ein, st, T, partial, lbt, unit);
   return cudaGetLastError();
 }
 
-template <typename S, typename M, int VE, int CPL>
-cudaError_t mass_modes(dim3 grid, cudaStream_t s, const void* Ein, const DevStep& st, const u64* T,
-                       const double2* Uv, const u64* mp, double* partial, int lbt, int unit) {
-#define RGS_MASS(MODE, NC) launch_mass<S, M, VE, CPL, MODE, NC>(grid, s, Ein, st, T, Uv, mp, partial, lbt, unit)
+// Positions that need the Gram pass: pair mode with two or four combos, merge mode.
+template <typename S, int VE, int CPL>
+cudaError_t gram_modes(dim3 grid, cudaStream_t s, const void* Ein, const DevStep& st, const u64* T, double* partial,
+                       int lbt, int unit) {
   if (st.mode == MODE_PAIR) {
-    if (st.ncombos == 1) return RGS_MASS(MODE_PAIR, 1);
-    if (st.ncombos == 2) return RGS_MASS(MODE_PAIR, 2);
-    return RGS_MASS(MODE_PAIR, 4);
+    if (st.ncombos == 2) return launch_gram<S, VE, CPL, MODE_PAIR, 2>(grid, s, Ein, st, T, partial, lbt, unit);
+    return launch_gram<S, VE, CPL, MODE_PAIR, 4>(grid, s, Ein, st, T, partial, lbt, unit);
   }
-  if (st.ncombos == 1) return RGS_MASS(MODE_MERGE, 1);
-  return RGS_MASS(MODE_MERGE, 2);
-#undef RGS_MASS
+  if (st.ncombos == 1) return launch_gram<S, VE, CPL, MODE_MERGE, 1>(grid, s, Ein, st, T, partial, lbt, unit);
+  return launch_gram<S, VE, CPL, MODE_MERGE, 2>(grid, s, Ein, st, T, partial, lbt, unit);
 }
 
-cudaError_t launch_mass_step(int precision, int Bt, int blocks, cudaStream_t s, const void* Ein, const DevStep& st,
-                             const u64* T, const double2* Uv, const u64* mp, double* partial, int unit) {
+cudaError_t launch_gram_step(int precision, int Bt, int blocks, cudaStream_t s, const void* Ein, const DevStep& st,
+                             const u64* T, double* partial, int unit) {
   const int lbt = __builtin_ctz((unsigned)Bt);
   const int VE = (precision != RGS_PREC_C128 && Bt >= 2) ? 2 : 1;
   const int lC = lbt - (VE == 2 ? 1 : 0);
   const int CPL = 1 << (lC - (lC < 5 ? lC : 5));
   const dim3 grid((unsigned)blocks);
   if (precision == RGS_PREC_C128) {
-    if (CPL == 1) return mass_modes<double, double, 1, 1>(grid, s, Ein, st, T, Uv, mp, partial, lbt, unit);
-    return mass_modes<double, double, 1, 2>(grid, s, Ein, st, T, Uv, mp, partial, lbt, unit);
+    if (CPL == 1) return gram_modes<double, 1, 1>(grid, s, Ein, st, T, partial, lbt, unit);
+    return gram_modes<double, 1, 2>(grid, s, Ein, st, T, partial, lbt, unit);
   }
-  if (precision == RGS_PREC_C64) {
-    if (VE == 1) return mass_modes<float, double, 1, 1>(grid, s, Ein, st, T, Uv, mp, partial, lbt, unit);
-    if (CPL == 1) return mass_modes<float, double, 2, 1>(grid, s, Ein, st, T, Uv, mp, partial, lbt, unit);
-    return mass_modes<float, double, 2, 2>(grid, s, Ein, st, T, Uv, mp, partial, lbt, unit);
-  }
-  if (VE == 1) return mass_modes<float, float, 1, 1>(grid, s, Ein, st, T, Uv, mp, partial, lbt, unit);
-  if (CPL == 1) return mass_modes<float, float, 2, 1>(grid, s, Ein, st, T, Uv, mp, partial, lbt, unit);
-  return mass_modes<float, float, 2, 2>(grid, s, Ein, st, T, Uv, mp, partial, lbt, unit);
+  if (VE == 1) return gram_modes<float, 1, 1>(grid, s, Ein, st, T, partial, lbt, unit);
+  if (CPL == 1) return gram_modes<float, 2, 1>(grid, s, Ein, st, T, partial, lbt, unit);
+  return gram_modes<float, 2, 2>(grid, s, Ein, st, T, partial, lbt, unit);
 }
 
 }  // namespace
 
-int chain_max_tile(int precision) { return precision == RGS_PREC_C128 ? 64 : 128; }
+int chain_max_tile(int precision) { return precision == RGS_PREC_C128 ? kChainMaxTile / 2 : kChainMaxTile; }
 
 int chain_layout(const Plan& plan, int Bt, int precision, ChainLayout& L) {
   if (Bt > chain_max_tile(precision)) return fail(RGS_ERR_ARG, "batch_tile above the chain sampler maximum");
@@ -304,7 +303,7 @@ int chain_layout(const Plan& plan, int Bt, int precision, ChainLayout& L) {
   if (rc) return rc;
   L.mass_blocks = kMassBlocks;
   L.off_partial = L.scan.total();
-  L.off_status = L.off_partial + align_up((size_t)L.mass_blocks * Bt * 2 * sizeof(double), 256);
+  L.off_status = L.off_partial + align_up((size_t)L.mass_blocks * Bt * 4 * sizeof(double), 256);
   L.total = L.off_status + 256;
   return RGS_OK;
 }
@@ -343,10 +342,12 @@ int chain_run(Plan& plan, const double* U, long long count, int mode_given, u64 
     for (int j = 0; j < plan.n; ++j) {
       const DevStep& st = plan.dev[j];
       const int v = st.v;
-      RGS_CUDA_TRY(launch_mass_step(precision, Bt, L.mass_blocks, stream, buf[j & 1], st, tables + st.table_off,
-                                    U2 + (size_t)v * 4, j ? maxbuf + (size_t)(j - 1) * Bt : nullptr, partial, j == 0));
+      const int analytic = (st.mode == MODE_PAIR && st.ncombos == 1) ? 1 : 0;
+      if (!analytic)
+        RGS_CUDA_TRY(launch_gram_step(precision, Bt, L.mass_blocks, stream, buf[j & 1], st, tables + st.table_off,
+                                      partial, j == 0));
       chain_decide_kernel<<<(Bt * 32 + 127) / 128, 128, 0, stream>>>(
-          partial, L.mass_blocks, Bt, cnt, j, v, U2, mode_given, bits, first, uniforms, plan.n, seed,
+          partial, L.mass_blocks, analytic, Bt, cnt, j, v, U2, mode_given, bits, first, uniforms, plan.n, seed,
           W + (size_t)j * Bt, out_logp, out_cond1, status);
       RGS_CUDA_TRY(cudaGetLastError());
       RGS_CUDA_TRY(scan_launch_step(precision, Bt, device, st, buf[j & 1], buf[(j + 1) & 1], tables + st.table_off,

@@ -9,8 +9,8 @@ namespace rgs {
 
 struct ChainLayout {
   ScanLayout scan;            // ping-pong tables, weights, maxima (as the scan executor)
-  int mass_blocks = 0;        // blocks of the branch-mass kernel
-  size_t off_partial = 0;     // per-block, per-item branch masses (float64)
+  int mass_blocks = 0;        // blocks of the Gram kernel
+  size_t off_partial = 0;     // per-block, per-item Gram matrices (4 float64)
   size_t off_status = 0;      // device status word
   size_t total = 0;
 };

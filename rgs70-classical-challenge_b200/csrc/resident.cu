@@ -9,9 +9,10 @@
 // different sizes and the two kinds of work share one launch:
 //   kind 0: amplitudes of given bitstrings (the streaming executor's arithmetic,
 //           bit for bit: same weights, same fma order, same renormalisation);
-//   kind 1: exact chain-rule samples (chain.cu's algorithm: both branch masses from one
-//           read of the table, inverse-CDF choice with the Philox uniform of
-//           (seed, item, position), then the chosen branch as one step).
+//   kind 1: exact chain-rule samples (chain.cu's algorithm: both branch masses from the
+//           position's Gram matrix, one read of the table, or in closed form; inverse-CDF
+//           choice with the Philox uniform of (seed, item, position); then the chosen
+//           branch as one step).
 // Table layout per block: E[c][b] (b fastest) for the unit's nb items.
 #include <cuda_runtime.h>
 
@@ -127,16 +128,62 @@ __device__ __forceinline__ void row_outputs(const typename Pair2<S>::T* __restri
   }
 }
 
+// Gram-matrix terms of row p0 for item b (chain_gram_kernel's accumulation).
+template <typename S>
+__device__ __forceinline__ void row_gram(const typename Pair2<S>::T* __restrict__ Ein, const DevStep& st, u64 p0,
+                                         int lnb, int b, bool unit, double& g0, double& g1, double& g2, double& g3) {
+  const u64 mask = (1ull << st.r_in) - 1ull;
+  double aar = 0.0, aai = 0.0, bar = 0.0, bai = 0.0, car = 0.0, cai = 0.0, dbr = 0.0, dbi = 0.0;
+  for (int k = 0; k < st.ncombos; ++k) {
+    const u64 p = p0 ^ st.combos[k];
+    const u64 cc = p & mask;
+    const int y = (int)((p >> st.r_in) & 1ull);
+    const int par = __popcll(cc & st.beta) & 1;
+    double er = 1.0, ei = 0.0;
+    if (!unit) {
+      const typename Pair2<S>::T e = Ein[(cc << lnb) + b];
+      er = (double)e.x;
+      ei = (double)e.y;
+    }
+    const double sr = par ? -er : er, si = par ? -ei : ei;
+    if (st.mode == MODE_PAIR && y) {
+      car += er;
+      cai += ei;
+      bar += sr;
+      bai += si;
+    } else {
+      aar += er;
+      aai += ei;
+      if (st.mode == MODE_PAIR) {
+        dbr += sr;
+        dbi += si;
+      } else {
+        bar += sr;
+        bai += si;
+      }
+    }
+  }
+  g0 = fma(aar, aar, fma(aai, aai, g0));
+  g1 = fma(bar, bar, fma(bai, bai, g1));
+  g2 = fma(aar, bar, fma(aai, bai, g2));
+  g3 = fma(aai, bar, fma(-aar, bai, g3));
+  if (st.mode == MODE_PAIR) {
+    g0 = fma(car, car, fma(cai, cai, g0));
+    g1 = fma(dbr, dbr, fma(dbi, dbi, g1));
+    g2 = fma(car, dbr, fma(cai, dbi, g2));
+    g3 = fma(cai, dbr, fma(-car, dbi, g3));
+  }
+}
+
 template <typename S, typename M>
 __global__ void __launch_bounds__(kResThreads, 1)
     resident_kernel(const ResInstance* __restrict__ insts, const ResWork* __restrict__ work, long long nwork,
                     int* __restrict__ counter) {
   typedef typename Pair2<S>::T V;
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ double red[kResThreads][2];
+  __shared__ double red[kResThreads][4];
   __shared__ u64 redm[kResThreads];
   __shared__ Cx<M> wA[kMaxResItems], wB[kMaxResItems];
-  __shared__ Cx<M> xw[2][2][kMaxResItems];  // [branch x][weight a/b][item]
   __shared__ ItemState ist[kMaxResItems];
   __shared__ DevStep sst;
   __shared__ long long s_unit;
@@ -184,47 +231,36 @@ __global__ void __launch_bounds__(kResThreads, 1)
       const u64 rows = mode == MODE_PAIR ? (1ull << (sst.r_out - 1)) : (1ull << sst.r_out);
 
       if (sample) {
-        // Both branches' masses (chain_mass_kernel), then the decision (chain_decide_kernel).
-        if (tid < nb) {
-          const double sc = ldexp(1.0, -scale_exponent(ist[tid].m2));
-          for (int x = 0; x < 2; ++x) {
-            Cx<M> a, c;
-            branch_weights<M>(U2[(v * 2 + x) * 2 + 0], U2[(v * 2 + x) * 2 + 1], sc, mode, 0, a, c);
-            if (tid >= wk.num) a = c = Cx<M>{(M)0, (M)0};
-            xw[x][0][tid] = a;
-            xw[x][1][tid] = c;
+        // Both branch masses from the position's Gram matrix (chain_gram_kernel), or in
+        // closed form on a one-combo pair position; then the decision (chain_decide_kernel).
+        const bool analytic = mode == MODE_PAIR && sst.ncombos == 1;
+        if (!analytic) {
+          double g0 = 0.0, g1 = 0.0, g2 = 0.0, g3 = 0.0;
+          for (u64 r = slot; r < rows; r += slots) {
+            const u64 ca = mode == MODE_PAIR ? deposit_zero(r, sst.pi) : r;
+            const u64 p0 = table_lookup(T, sst.nbytes, ca);
+            row_gram<S>(Ein, sst, p0, lnb, b, unit, g0, g1, g2, g3);
           }
+          red[tid][0] = g0;
+          red[tid][1] = g1;
+          red[tid][2] = g2;
+          red[tid][3] = g3;
         }
         __syncthreads();
-        double acc0 = 0.0, acc1 = 0.0;
-        for (u64 r = slot; r < rows; r += slots) {
-          const u64 ca = mode == MODE_PAIR ? deposit_zero(r, sst.pi) : r;
-          const u64 p0 = table_lookup(T, sst.nbytes, ca);
-#pragma unroll
-          for (int x = 0; x < 2; ++x) {
-            Cx<M> oa, ob;
-            row_outputs<S, M>(Ein, sst, p0, lnb, b, unit, xw[x][0][b], xw[x][1][b], 0, 0, oa, ob);
-            const S ar = (S)oa.re, ai = (S)oa.im;
-            double m = (double)norm2(ar, ai);
-            if (mode == MODE_PAIR) {
-              const S br = (S)ob.re, bi = (S)ob.im;
-              m += (double)norm2(br, bi);
+        if (tid < nb) {
+          double g0 = 1.0, g1 = 1.0, g2 = 0.0, g3 = 0.0;
+          if (!analytic) {
+            g0 = g1 = 0.0;
+            for (int k = 0; k < slots; ++k) {
+              const double* q = red[tid + (k << lnb)];
+              g0 += q[0];
+              g1 += q[1];
+              g2 += q[2];
+              g3 += q[3];
             }
-            if (x)
-              acc1 += m;
-            else
-              acc0 += m;
           }
-        }
-        red[tid][0] = acc0;
-        red[tid][1] = acc1;
-        __syncthreads();
-        if (tid < nb) {
-          double m0 = 0.0, m1 = 0.0;
-          for (int k = 0; k < slots; ++k) {
-            m0 += red[tid + (k << lnb)][0];
-            m1 += red[tid + (k << lnb)][1];
-          }
+          const double m0 = branch_mass(U2 + (v * 2 + 0) * 2, g0, g1, g2, g3);
+          const double m1 = branch_mass(U2 + (v * 2 + 1) * 2, g0, g1, g2, g3);
           ItemState& s = ist[tid];
           int x = 0;
           if (tid < wk.num) {
@@ -243,8 +279,12 @@ __global__ void __launch_bounds__(kResThreads, 1)
                 s.hi |= 1ull << (v - 64);
             }
           }
-          wA[tid] = xw[x][0][tid];
-          wB[tid] = xw[x][1][tid];
+          const double sc = ldexp(1.0, -scale_exponent(s.m2));
+          Cx<M> a, c;
+          branch_weights<M>(U2[(v * 2 + x) * 2 + 0], U2[(v * 2 + x) * 2 + 1], sc, mode, 0, a, c);
+          if (tid >= wk.num) a = c = Cx<M>{(M)0, (M)0};
+          wA[tid] = a;
+          wB[tid] = c;
           s.flags = 0;
           if (!s.done) s.esum += scale_exponent(s.m2);
         }

@@ -108,6 +108,16 @@ __device__ __forceinline__ int scale_exponent(double m2) {
   return e;
 }
 
+// Mass of one branch of a position from the position's Gram matrix G (chain rule):
+// u = U_v[x, :] (two complex128), M = G00 |u0|^2 + G11 |u1|^2 + 2 Re(G01 u0 conj(u1)),
+// clamped at zero against rounding.
+__device__ __forceinline__ double branch_mass(const double2* u, double g00, double g11, double g01r, double g01i) {
+  const double2 a = u[0], c = u[1];
+  const double zr = a.x * c.x + a.y * c.y, zi = a.y * c.x - a.x * c.y;
+  const double m = g00 * (a.x * a.x + a.y * a.y) + g11 * (c.x * c.x + c.y * c.y) + 2.0 * (g01r * zr - g01i * zi);
+  return m > 0.0 ? m : 0.0;
+}
+
 // Maximum-slot encoding: non-negative floats (complex64 tables) or doubles
 // (complex128 tables) as their IEEE bits, so unsigned max is float max.
 template <typename S>
