@@ -199,6 +199,9 @@ void build_device(Plan& p) {
       d.mode = MODE_PAIR;
       d.t = (unsigned long long)st.ycol;
       d.pi = highest_bit(st.ycol);
+      // Combos with y bit 0 first (stable): the step kernel assigns the two output rows
+      // of a pair by the y bit of the row's own image alone.
+      std::stable_partition(combos.begin(), combos.end(), [&](u128 c) { return !bit_of(c, st.r_in); });
     } else {
       // e_y lies in the kernel: keep one representative per y pair (the one with y bit 0).
       d.mode = MODE_MERGE;
@@ -210,6 +213,9 @@ void build_device(Plan& p) {
       combos.swap(reps);
     }
     d.ncombos = (int)combos.size();
+    d.ng0 = 0;
+    for (auto c : combos)
+      if (!bit_of(c, st.r_in)) ++d.ng0;
     for (int k = 0; k < 4; ++k) d.combos[k] = k < d.ncombos ? (unsigned long long)combos[k] : 0ull;
     p.dev.push_back(d);
   }

@@ -54,6 +54,7 @@ struct DevStep {
   unsigned long long combos[4];  // MODE_PAIR/FIXED: span(kernel); MODE_MERGE: y-bit-0 representatives
   unsigned long long table_off;  // offset (in u64) of this step's byte tables in the table blob
   int r_in, r_out, nbytes, ncombos, mode, pi, v, fixed;
+  int ng0;                       // MODE_PAIR: the first ng0 combos have y bit 0 (the rest y bit 1)
 };
 
 struct Plan {

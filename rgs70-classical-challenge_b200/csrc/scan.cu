@@ -214,29 +214,31 @@ int scan_layout(const Plan& plan, int Bt, int precision, ScanLayout& L) {
 
 namespace {
 
-template <typename S, typename M, int VE, int CPL, int MODE, int NC>
+template <typename S, typename M, int VE, int CPL, int MODE, int NC, int NG0>
 cudaError_t launch_row(dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevStep& st, const u64* T,
                        const double4* W, const unsigned char* F, const u64* mp, u64* mc, int lbt, int unit) {
-  scan_row_kernel<S, M, VE, MODE, NC, CPL><<<grid, 256, 0, s>>>((const S*)Ein, (S*)Eout, st, T, W, F, mp, mc, lbt,
-                                                                unit);
+  scan_row_kernel<S, M, VE, MODE, NC, CPL, NG0><<<grid, 256, 0, s>>>((const S*)Ein, (S*)Eout, st, T, W, F, mp, mc,
+                                                                     lbt, unit);
   return cudaGetLastError();
 }
 
 template <typename S, typename M, int VE, int CPL>
 cudaError_t launch_modes(dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevStep& st, const u64* T,
                          const double4* W, const unsigned char* F, const u64* mp, u64* mc, int lbt, int unit) {
-#define RGS_ROW(MODE, NC) launch_row<S, M, VE, CPL, MODE, NC>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit)
+#define RGS_ROW(MODE, NC, NG0) \
+  launch_row<S, M, VE, CPL, MODE, NC, NG0>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit)
   if (st.mode == MODE_PAIR) {
-    if (st.ncombos == 1) return RGS_ROW(MODE_PAIR, 1);
-    if (st.ncombos == 2) return RGS_ROW(MODE_PAIR, 2);
-    return RGS_ROW(MODE_PAIR, 4);
+    // The combos with kappa = 0 come first: all of them, or half (kappa is linear in the combo).
+    if (st.ncombos == 1) return RGS_ROW(MODE_PAIR, 1, 1);
+    if (st.ncombos == 2) return st.ng0 == 2 ? RGS_ROW(MODE_PAIR, 2, 2) : RGS_ROW(MODE_PAIR, 2, 1);
+    return st.ng0 == 4 ? RGS_ROW(MODE_PAIR, 4, 4) : RGS_ROW(MODE_PAIR, 4, 2);
   }
   if (st.mode == MODE_MERGE) {
-    if (st.ncombos == 1) return RGS_ROW(MODE_MERGE, 1);
-    return RGS_ROW(MODE_MERGE, 2);
+    if (st.ncombos == 1) return RGS_ROW(MODE_MERGE, 1, 1);
+    return RGS_ROW(MODE_MERGE, 2, 2);
   }
-  if (st.ncombos == 1) return RGS_ROW(MODE_FIXED, 1);
-  return RGS_ROW(MODE_FIXED, 2);
+  if (st.ncombos == 1) return RGS_ROW(MODE_FIXED, 1, 1);
+  return RGS_ROW(MODE_FIXED, 2, 2);
 #undef RGS_ROW
 }
 

@@ -9,12 +9,20 @@
 //
 // Modes (see plan.hpp): PAIR writes rows c' and c'^t from the same NC gathered rows;
 // MERGE and FIXED write one row.  The per-item weight pair (wA, wB) is prepared per
-// mode so the inner loop is select + complex FMA:
+// mode so that the inner loop is a complex FMA:
 //   PAIR : wA = f(0) s, wB = f(1) s       row c'  : y ? wB : wA, negated iff y & par
 //                                          row c'^t: y ? wA : wB, negated iff !y & par
 //   MERGE: wA = (f0 + f1) s, wB = (f0 - f1) s        par ? wB : wA
 //   FIXED: wA = f(y) s                              negated iff y & par
 // with par = popc(c & beta) ^ ov and s = 2^-e the renormalisation of gpu_kernel.py:146-148.
+//
+// PAIR without per-item selects.  The y bit of gather k is y_k = y(p0) ^ kappa_k, where
+// kappa_k is bit r_in of combo k, a constant of the step; the compiler orders the combos
+// with kappa = 0 first (NG0 of them).  With X = sum_{k<NG0} e wA + sum_{k>=NG0} (-1)^par e wB
+// and Y = sum_{k<NG0} (-1)^par e wB + sum_{k>=NG0} e wA, row c' receives X and row c'^t
+// receives Y when y(p0) = 0, and the other way round when y(p0) = 1: the choice is one
+// swap of the two store addresses per row, and the sign is applied to the gathered value
+// (exactly the negated product), so no weight is selected per item.
 #pragma once
 #include "scan_device.cuh"
 
@@ -31,7 +39,15 @@ struct LoadsInFlight {
   static constexpr int value = sizeof(M) > sizeof(S) ? 4 : 8;
 };
 
-template <typename S, typename M, int VE, int MODE, int NC, int CPL>
+// x with its sign flipped iff neg (exact).
+__device__ __forceinline__ float flip_sign(float x, int neg) {
+  return __int_as_float(__float_as_int(x) ^ (neg << 31));
+}
+__device__ __forceinline__ double flip_sign(double x, int neg) {
+  return __hiloint2double(__double2hiint(x) ^ (neg << 31), __double2loint(x));
+}
+
+template <typename S, typename M, int VE, int MODE, int NC, int CPL, int NG0>
 __global__ void __launch_bounds__(256, 2) scan_row_kernel(const S* __restrict__ Ein, S* __restrict__ Eout,
                                                        const __grid_constant__ DevStep st,
                                                        const u64* __restrict__ T, const double4* __restrict__ W,
@@ -98,7 +114,7 @@ __global__ void __launch_bounds__(256, 2) scan_row_kernel(const S* __restrict__ 
   for (u64 base = warp * per_iter; base < items; base += nwarps * per_iter) {
     u64 ca[U], cb[U];
     u64 cc[U][NC];
-    int yy[U][NC], pc[U][NC];
+    int pc[U][NC];
     bool ok[U];
     Chunk<S, VE> e[U][NC][CPL];
 #pragma unroll
@@ -113,11 +129,15 @@ __global__ void __launch_bounds__(256, 2) scan_row_kernel(const S* __restrict__ 
         cb[u] = it;
       }
       const u64 p0 = ok[u] ? table_lookup(T, st.nbytes, ca[u]) : 0ull;
+      if (MODE == MODE_PAIR && ((p0 >> st.r_in) & 1ull)) {  // y(p0) = 1: swap the two output rows
+        const u64 tmp = ca[u];
+        ca[u] = cb[u];
+        cb[u] = tmp;
+      }
 #pragma unroll
       for (int k = 0; k < NC; ++k) {
         const u64 p = p0 ^ st.combos[k];
         cc[u][k] = p & mask;
-        yy[u][k] = (int)((p >> st.r_in) & 1ull);
         pc[u][k] = __popcll(cc[u][k] & st.beta) & 1;
       }
     }
@@ -147,25 +167,22 @@ __global__ void __launch_bounds__(256, 2) scan_row_kernel(const S* __restrict__ 
           Cx<M> oa{(M)0, (M)0}, ob{(M)0, (M)0};
 #pragma unroll
           for (int k = 0; k < NC; ++k) {
-            const M er = (M)e[u][k][j].re(v), ei = (M)e[u][k][j].im(v);
             const int par = pc[u][k] ^ ov[i];
             if (MODE == MODE_PAIR) {
-              const int y = yy[u][k];
-              Cx<M> wa = y ? wB[i] : wA[i];
-              Cx<M> wb = y ? wA[i] : wB[i];
-              if (y & par) {
-                wa.re = -wa.re;
-                wa.im = -wa.im;
+              const M pr = (M)e[u][k][j].re(v), pi = (M)e[u][k][j].im(v);
+              const M nr = flip_sign(pr, par), ni = flip_sign(pi, par);
+              if (k < NG0) {
+                cmad(oa, pr, pi, wA[i]);
+                cmad(ob, nr, ni, wB[i]);
+              } else {
+                cmad(oa, nr, ni, wB[i]);
+                cmad(ob, pr, pi, wA[i]);
               }
-              if ((y ^ 1) & par) {
-                wb.re = -wb.re;
-                wb.im = -wb.im;
-              }
-              cmad(oa, er, ei, wa);
-              cmad(ob, er, ei, wb);
             } else if (MODE == MODE_MERGE) {
+              const M er = (M)e[u][k][j].re(v), ei = (M)e[u][k][j].im(v);
               cmad(oa, er, ei, par ? wB[i] : wA[i]);
             } else {
+              const M er = (M)e[u][k][j].re(v), ei = (M)e[u][k][j].im(v);
               Cx<M> w = wA[i];
               if (yf[i] & par) {
                 w.re = -w.re;
