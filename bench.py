@@ -652,6 +652,7 @@ def run_rgs70(args, rank, world, local_rank):
     born = json.loads((ROOT / "tests" / "golden" / "rgs70_born.json").read_text())["probability_c128"]
     g, u = fx["rgs70/graph"], fx["rgs70/measurement_unitaries"]
     frozen, optimised = fx["rgs70/scan_order"].tolist(), fx["rgs70/scan_order_optimized"].tolist()
+    searched = json.loads((ROOT / "tests" / "golden" / "searched_orders.json").read_text())["rgs70"]["order"]
     rows = rec["benchmark_rows"]
     bits = np.array([[int(c) for c in r["bitstring_q0_left"]] for r in rows], dtype=np.uint8)
     ref_p = np.array([r["probability_c128"] for r in rows])
@@ -672,7 +673,6 @@ def run_rgs70(args, rank, world, local_rank):
         torch.cuda.empty_cache()
 
     plan_f = pkg.ScanPlan(70, pkg.edges_from_graph(g), frozen)
-    plan_o = pkg.ScanPlan(70, pkg.edges_from_graph(g), optimised)
     d_bits = torch.from_numpy(pkg.pack_bits(bits, 70).view(np.int64)).to(device)
     legs = {}
     with ClockSampler(local_rank) as clocks:
@@ -689,33 +689,49 @@ def run_rgs70(args, rank, world, local_rank):
                           "achieved_GBps": step_bytes(plan_f.ranks, esize) * len(bits) * args.steps / t / 1e9}
             del eng, val, ls
             free()
-        # Exact Born samples, optimised order, complex64 tables, 8 samples per tile.
+        # Exact Born samples, complex64 tables, 8 samples per tile: the reference's optimised
+        # order, then the order found by this package's search (tests/golden/searched_orders.json).
         S = 16
-        cs = pkg.ChainSampler(g, u, optimised, device=device, precision="c64", batch_tile=8)
-        outs = cs._outs(S)
-        seed = [70000 + 1000 * rank]
+        sampled = {}
+        for name, sorder in (("reference_optimised", optimised), ("searched", searched)):
+            cs = pkg.ChainSampler(g, u, sorder, device=device, precision="c64", batch_tile=8)
+            outs = cs._outs(S)
+            seed = [70000 + 1000 * rank]
 
-        def sample():
-            seed[0] += 1
-            return cs.sample_device(S, seed=seed[0], check=False, stream=stream, outs=outs)
-        sample()
-        ts = timed(sample, args.steps)
-        sbits, sval, sls, slogp = sample()
-        torch.cuda.synchronize(device)
-        samples = pkg.unpack_bits(sbits.cpu().numpy(), 70)
-        p64 = np.abs(pkg.amplitudes_from(sval.cpu().numpy().astype(np.complex128), sls.cpu().numpy(), 70)) ** 2
-        lp = slogp.cpu().numpy()
-        del cs, outs, sbits, sval, sls, slogp
-        free()
-    so = pkg.ScanOracle(g, u, optimised, device=device, fp64=True, batch_tile=4)
-    p128 = so.probabilities(samples)
+            def sample():
+                seed[0] += 1
+                return cs.sample_device(S, seed=seed[0], check=False, stream=stream, outs=outs)
+            sample()
+            ts = timed(sample, args.steps)
+            sbits, sval, sls, slogp = sample()
+            torch.cuda.synchronize(device)
+            sampled[name] = {"t": ts, "plan": cs.plan, "bits": pkg.unpack_bits(sbits.cpu().numpy(), 70),
+                             "p64": np.abs(pkg.amplitudes_from(sval.cpu().numpy().astype(np.complex128),
+                                                               sls.cpu().numpy(), 70)) ** 2,
+                             "logp": slogp.cpu().numpy()}
+            del cs, outs, sbits, sval, sls, slogp
+            free()
+    so = pkg.ScanOracle(g, u, searched, device=device, fp64=True, batch_tile=4)
+    for rec_s in sampled.values():
+        rec_s["p128"] = so.probabilities(rec_s["bits"])
     del so
     free()
-    sample_bytes = chain_bytes(plan_o, 8)
-    z = p128 * 2.0 ** 70
     zref = np.concatenate([born["batch1"], born["batch2"]]) * 2.0 ** 70
-    ks = stats.ks_2samp(z, zref)
-    rate_s = S * args.steps / ts
+    samples_out = {}
+    for name, rec_s in sampled.items():
+        rate = S * args.steps / rec_s["t"]
+        z = rec_s["p128"] * 2.0 ** 70
+        ks = stats.ks_2samp(z, zref)
+        samples_out[name] = {
+            "value": rate, "unit": "samples/s", "sum_states": rec_s["plan"].sum_states,
+            "rmax": rec_s["plan"].rmax, "samples_per_step": S,
+            "vs_reference_2xH200": rate / RGS70_REF_SAMPLES_PER_S_2GPU,
+            "achieved_GBps": chain_bytes(rec_s["plan"], 8) * S * args.steps / rec_s["t"] / 1e9,
+            "max_rel_err_c64_vs_c128_rescore": float(np.max(np.abs(rec_s["p64"] - rec_s["p128"]) / rec_s["p128"])),
+            "max_abs_logp_minus_log_p128": float(np.max(np.abs(rec_s["logp"] - np.log(rec_s["p128"])))),
+            "linear_xeb_of_these_samples": float(z.mean() - 1),
+            "ks_vs_reference_born_samples": {"statistic": float(ks.statistic), "pvalue": float(ks.pvalue),
+                                             "reference_samples": int(len(zref))}}
     peaks_path = ROOT / "MEASURED_PEAKS.json"
     peak = float(json.loads(peaks_path.read_text())["hbm_gbs"]) if peaks_path.exists() else 6650.0
     value = legs["c64"]["amplitudes_per_s"]
@@ -732,15 +748,7 @@ def run_rgs70(args, rank, world, local_rank):
             "reference_published": {"c64_amplitudes_per_s_1xH200": RGS70_REF_C64_AMP_PER_S,
                                     "c128_amplitudes_per_s_1xH200": RGS70_REF_C128_AMP_PER_S,
                                     "born_samples_per_s_2xH200": RGS70_REF_SAMPLES_PER_S_2GPU},
-            "exact_born_samples": {
-                "value": rate_s, "unit": "samples/s", "order": "optimised (sum 2^r 7,919,632,381)",
-                "samples_per_step": S, "vs_reference_2xH200": rate_s / RGS70_REF_SAMPLES_PER_S_2GPU,
-                "achieved_GBps": sample_bytes * S * args.steps / ts / 1e9,
-                "max_rel_err_c64_vs_c128_rescore": float(np.max(np.abs(p64 - p128) / p128)),
-                "max_abs_logp_minus_log_p128": float(np.max(np.abs(lp - np.log(p128)))),
-                "linear_xeb_of_these_samples": float(z.mean() - 1),
-                "ks_vs_reference_born_samples": {"statistic": float(ks.statistic), "pvalue": float(ks.pvalue),
-                                                 "reference_samples": int(len(zref))}},
+            "exact_born_samples": samples_out,
             "gpu_launches": args.steps * -(-len(bits) // 8) * (70 + 2), "clocks": clocks.summary()}
     if rank == 0:
         print(json.dumps(line), flush=True)

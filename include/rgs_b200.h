@@ -78,6 +78,17 @@ int rgs_plan_step_tables(const rgs_plan* plan, int32_t j, uint64_t* tables, int3
 int rgs_rank_profile(int32_t n, int32_t n_edges, const int32_t* edges, const int32_t* order,
                      const uint8_t* fixed, int32_t* ranks);
 
+/* Scan-order search: simulated annealing over orders for the cost sum_j 2^{r_j} (the
+ * table entries of one sweep) subject to max_j r_j <= max_rank (max_rank < 0: the
+ * starting order's peak).  Replaces W/order_optimization/search.cpp:33-68 (same four move
+ * kinds and peak constraint) for any n <= 128, with an iteration budget instead of a
+ * wall-clock one and `threads` independent chains (the best wins); deterministic for a
+ * seed.  order_out: int32[n]; ranks_out: int32[n] or NULL; cost_out or NULL.  Plans
+ * without fixed vertices.  Host-only. */
+int rgs_order_search(int32_t n, int32_t n_edges, const int32_t* edges, const int32_t* order, int32_t max_rank,
+                     int64_t iterations, uint64_t seed, int32_t threads, int32_t* order_out, int32_t* ranks_out,
+                     double* cost_out);
+
 /* ---------------------------------------------------------------- scan executor
  * Replaces GPUMixin.alloc/_sweep (W/upstream_scan/gpu_kernel.py:111-170,
  * gpu_kernel_fp64.py:76-135) and ScanOracle.amplitude (W/scan_oracle.py:25-29),

@@ -146,6 +146,27 @@ int rgs_rank_profile(int32_t n, int32_t n_edges, const int32_t* edges, const int
   return RGS_OK;
 }
 
+int rgs_order_search(int32_t n, int32_t n_edges, const int32_t* edges, const int32_t* order, int32_t max_rank,
+                     int64_t iterations, uint64_t seed, int32_t threads, int32_t* order_out, int32_t* ranks_out,
+                     double* cost_out) {
+  std::vector<std::pair<int, int>> e;
+  std::vector<int> o;
+  std::vector<uint8_t> f;
+  int rc = read_graph(n, n_edges, edges, order, nullptr, e, o, f);
+  if (rc) return rc;
+  if (!order_out) return fail(RGS_ERR_ARG, "order_out is required");
+  if (iterations < 0) return fail(RGS_ERR_ARG, "iterations must be >= 0");
+  std::vector<int> best, ranks;
+  double cost = 0.0;
+  std::string err = order_search(n, e, o, max_rank, iterations, seed, threads, best, ranks, cost);
+  if (!err.empty()) return fail(RGS_ERR_ARG, err);
+  for (int i = 0; i < n; ++i) order_out[i] = best[i];
+  if (ranks_out)
+    for (int i = 0; i < n; ++i) ranks_out[i] = ranks[i];
+  if (cost_out) *cost_out = cost;
+  return RGS_OK;
+}
+
 int rgs_scan_max_batch_tile(int32_t precision, int32_t* tile) {
   if (!tile) return fail(RGS_ERR_ARG, "tile is NULL");
   if (precision < RGS_PREC_C64 || precision > RGS_PREC_C128) return fail(RGS_ERR_ARG, "unknown precision");

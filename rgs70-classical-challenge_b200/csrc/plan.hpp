@@ -99,6 +99,14 @@ std::vector<u128> future_masks(int n, const std::vector<std::pair<int, int>>& ed
 std::string rank_profile(int n, const std::vector<std::pair<int, int>>& edges, const std::vector<int>& order,
                          const std::vector<uint8_t>& fixed, std::vector<int>& ranks);
 
+// Scan-order search (order_search.cpp): annealing over orders for sum_j 2^{r_j} under
+// max r_j <= max_rank (< 0: the starting order's), `threads` independent chains of
+// `iterations` proposals each; deterministic for (seed, threads, iterations).  Plans
+// without fixed vertices.  Returns an empty string on success, else an error message.
+std::string order_search(int n, const std::vector<std::pair<int, int>>& edges, const std::vector<int>& start,
+                         int max_rank, long long iterations, uint64_t seed, int threads, std::vector<int>& best_order,
+                         std::vector<int>& best_ranks, double& best_cost);
+
 // Byte tables of one step: out[b * 256 + value] = XOR of lcols[8 b + t] over set bits t of value.
 void byte_tables(const std::vector<u128>& cols, int nbits, std::vector<u128>& out, int& nbytes);
 

@@ -11,7 +11,7 @@ import numpy as np
 
 from . import _lib
 
-__all__ = ["Step", "ScanPlan", "make_plan", "future_masks", "rank_profile", "byte_tables", "kernel_combos",
+__all__ = ["Step", "ScanPlan", "make_plan", "future_masks", "rank_profile", "search_order", "byte_tables", "kernel_combos",
            "edges_from_graph"]
 
 
@@ -161,6 +161,21 @@ def rank_profile(N, edges, order, fixed=frozenset()):
                                            None if f is None else _lib.ptr(f, ctypes.c_uint8),
                                            _lib.ptr(r, ctypes.c_int32)))
     return r.tolist()
+
+
+def search_order(N, edges, order, max_rank=None, iterations=100000, seed=0, threads=1):
+    """Scan-order search (``W/order_optimization/search.cpp``): annealed order minimising
+    sum_j 2^{r_j} with max r_j <= max_rank (default: the starting order's peak).
+    Returns (order, ranks, cost)."""
+    e, o, _ = _graph_args(int(N), edges, order, frozenset())
+    out = np.zeros(int(N), dtype=np.int32)
+    ranks = np.zeros(int(N), dtype=np.int32)
+    cost = ctypes.c_double()
+    _lib.check(_lib.lib().rgs_order_search(int(N), len(e), _lib.ptr(e, ctypes.c_int32), _lib.ptr(o, ctypes.c_int32),
+                                           -1 if max_rank is None else int(max_rank), int(iterations),
+                                           int(seed) & (2 ** 64 - 1), int(threads), _lib.ptr(out, ctypes.c_int32),
+                                           _lib.ptr(ranks, ctypes.c_int32), ctypes.byref(cost)))
+    return out.tolist(), ranks.tolist(), float(cost.value)
 
 
 def byte_tables(cols, nbits):
