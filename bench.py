@@ -199,21 +199,35 @@ def run_ours(args, rank, world, local_rank):
     rng = np.random.default_rng(BITS_SEED + rank)
     bits = pkg.instances.uniform_bits(BATCH, N_QUBITS, rng)
     packed = pkg.pack_bits(bits, N_QUBITS)
-    tile64 = min(args.tile64, 1 << max(0, (BATCH - 1).bit_length()))
+    bulk_tile = args.tile64 or (256 if args.bulk == "c64f32" else 128)
+    tile64 = min(bulk_tile, 1 << max(0, (BATCH - 1).bit_length()))
     tile128 = min(args.tile128, 1 << max(0, (BATCH - 1).bit_length()))
     use64, use128 = args.only in ("both", "c64"), args.only in ("both", "c128")
-    eng64 = pkg.ScanEngine(plan, inst.u, device=device, precision="c64", batch_tile=tile64) if use64 else None
+    eng64 = pkg.ScanEngine(plan, inst.u, device=device, precision=args.bulk, batch_tile=tile64) if use64 else None
     eng128 = pkg.ScanEngine(plan, inst.u, device=device, precision="c128", batch_tile=tile128) if use128 else None
     d_bits = torch.from_numpy(packed.view(np.int64)).to(device)
     v64, l64 = eng64.out_tensors(BATCH) if use64 else (None, None)
     v128, l128 = eng128.out_tensors(BATCH) if use128 else (None, None)
     stream = torch.cuda.current_stream(device)
 
-    def device_step():
+    def queue_step(s):
         if use64:
-            eng64.run_bits(d_bits, v64, l64, stream=stream)
+            eng64.run_bits(d_bits, v64, l64, stream=s)
         if use128:
-            eng128.run_bits(d_bits, v128, l128, stream=stream)
+            eng128.run_bits(d_bits, v128, l128, stream=s)
+
+    # One sweep eagerly (allocates the workspaces), then the step as a CUDA graph: the
+    # 42 launches per tile replay without host launch overhead.
+    queue_step(stream)
+    torch.cuda.synchronize(device)
+    graphs = {"step": pkg.capture_graph(device, queue_step)}
+    if use64:
+        graphs["bulk"] = pkg.capture_graph(device, lambda s: eng64.run_bits(d_bits, v64, l64, stream=s))
+    if use128:
+        graphs["recheck"] = pkg.capture_graph(device, lambda s: eng128.run_bits(d_bits, v128, l128, stream=s))
+
+    def device_step():
+        graphs["step"].replay()
 
     def barrier():
         if world > 1:
@@ -244,8 +258,22 @@ def run_ours(args, rank, world, local_rank):
     with ClockSampler(local_rank) as clocks:
         t_step = timed(device_step, args.steps)
     # Split of the step, and the FP64 recheck error (per result: max and quantiles).
-    t64 = timed(lambda: eng64.run_bits(d_bits, v64, l64, stream=stream), args.steps) if use64 else None
-    t128 = timed(lambda: eng128.run_bits(d_bits, v128, l128, stream=stream), args.steps) if use128 else None
+    t64 = timed(graphs["bulk"].replay, args.steps) if use64 else None
+    t128 = timed(graphs["recheck"].replay, args.steps) if use128 else None
+    # The other complex64 recipe (float64 arithmetic on complex64 tables, the reference's
+    # own kernel recipe), for comparison: time and error only.
+    alt = None
+    if use64 and use128 and not args.no_alt:
+        alt_prec = "c64" if args.bulk == "c64f32" else "c64f32"
+        alt_tile = min(256 if alt_prec == "c64f32" else 128, 1 << max(0, (BATCH - 1).bit_length()))
+        eng_alt = pkg.ScanEngine(plan, inst.u, device=device, precision=alt_prec, batch_tile=alt_tile)
+        va, la = eng_alt.out_tensors(BATCH)
+        eng_alt.run_bits(d_bits, va, la, stream=stream)
+        torch.cuda.synchronize(device)
+        g_alt = pkg.capture_graph(device, lambda s: eng_alt.run_bits(d_bits, va, la, stream=s))
+        t_alt = timed(g_alt.replay, args.steps)
+        alt = {"precision": alt_prec, "t": t_alt, "v": va, "l": la}
+        del g_alt, eng_alt
     recheck = None
     p128 = None
     if use64 and use128:
@@ -253,13 +281,20 @@ def run_ours(args, rank, world, local_rank):
         p128 = np.abs(pkg.amplitudes_from(v128.cpu().numpy(), l128.cpu().numpy(), N_QUBITS)) ** 2
         if not (np.all(np.isfinite(p64)) and np.all(np.isfinite(p128))):
             raise ArithmeticError("non-finite probability in the benchmark run")
-        rel = np.abs(p64 - p128) / p128
-        scaled = np.abs(p64 - p128) * 2.0 ** N_QUBITS
-        recheck = {"max_prob_rel_err": float(rel.max()), "median_prob_rel_err": float(np.median(rel)),
-                   "p999_prob_rel_err": float(np.quantile(rel, 0.999)),
-                   "frac_above_1e-4": float(np.mean(rel > 1e-4)),
-                   "max_rel_err_p_ge_0.01_over_2^n": float(rel[p128 * 2.0 ** N_QUBITS >= 0.01].max()),
-                   "max_abs_err_times_2^n": float(scaled.max())}
+        def err_stats(p):
+            rel = np.abs(p - p128) / p128
+            scaled = np.abs(p - p128) * 2.0 ** N_QUBITS
+            return {"max_prob_rel_err": float(rel.max()), "median_prob_rel_err": float(np.median(rel)),
+                    "p999_prob_rel_err": float(np.quantile(rel, 0.999)),
+                    "frac_above_1e-4": float(np.mean(rel > 1e-4)),
+                    "max_rel_err_p_ge_0.01_over_2^n": float(rel[p128 * 2.0 ** N_QUBITS >= 0.01].max()),
+                    "max_abs_err_times_2^n": float(scaled.max())}
+        recheck = {"bulk": args.bulk, **err_stats(p64)}
+        if alt is not None:
+            pa = np.abs(pkg.amplitudes_from(alt["v"].cpu().numpy(), alt["l"].cpu().numpy(), N_QUBITS)) ** 2
+            recheck["other_complex64_recipe"] = {"precision": alt["precision"],
+                                                 "amplitudes_per_s": world * BATCH * args.steps / alt["t"],
+                                                 **err_stats(pa)}
 
     # End to end through the public API: pinned host bits in, host probabilities out.
     h_bits = torch.from_numpy(packed.view(np.int64)).pin_memory()
@@ -300,9 +335,10 @@ def run_ours(args, rank, world, local_rank):
     traffic_path = ROOT / "profiles" / "scan_step_traffic.json"
     if traffic_path.exists():
         tr = json.loads(traffic_path.read_text())["dram_bytes_per_tile"]
-        if (not use64 or tr["c64"]["tile"] == tile64) and (not use128 or tr["c128"]["tile"] == tile128):
-            traffic = ((math.ceil(BATCH / tile64) * tr["c64"]["bytes"] if use64 else 0)
-                       + (math.ceil(BATCH / tile128) * tr["c128"]["bytes"] if use128 else 0))
+        t64r, t128r = tr.get(args.bulk), tr.get("c128")
+        if (not use64 or (t64r and t64r["tile"] == tile64)) and (not use128 or (t128r and t128r["tile"] == tile128)):
+            traffic = ((math.ceil(BATCH / tile64) * t64r["bytes"] if use64 else 0)
+                       + (math.ceil(BATCH / tile128) * t128r["bytes"] if use128 else 0))
     groups64 = math.ceil(BATCH / tile64) if use64 else 0
     groups128 = math.ceil(BATCH / tile128) if use128 else 0
     launches = args.steps * ((groups64 + groups128) * (N_QUBITS + 2))
@@ -333,11 +369,15 @@ def run_ours(args, rank, world, local_rank):
             "config": {"workload": "single-instance throughput: n=40 random 3-regular, Haar SU(2), "
                                    "65536 uniform 40-bit strings, complex64 + FP64 recheck of every result",
                        "instance": inst.name, "rmax": inst.rmax, "sum_states": inst.sum_states,
-                       "batch_per_gpu": BATCH, "batch_tile": {"c64": tile64, "c128": tile128},
+                       "batch_per_gpu": BATCH, "batch_tile": {args.bulk: tile64, "c128": tile128},
                        "precisions": args.only,
+                       "bulk": ("complex64 tables, float32 arithmetic" if args.bulk == "c64f32"
+                                else "complex64 tables, float64 arithmetic (the reference recipe)"),
+                       "recheck": "complex128 tables, float64 arithmetic, every result",
+                       "launch": "each precision's sweep replayed from a CUDA graph",
                        "l2": "inputs larger than L2 (tables of 2^20 rows x batch tile, >= 2 x 1 GiB)",
                        "parallelism": f"replicas x{world}"},
-            "split": {"c64_amplitudes_per_s": world * BATCH * args.steps / t64 if t64 else None,
+            "split": {f"{args.bulk}_amplitudes_per_s": world * BATCH * args.steps / t64 if t64 else None,
                       "c128_amplitudes_per_s": world * BATCH * args.steps / t128 if t128 else None},
             "fp64_recheck": recheck,
             "exact_born_samples": {"value": chain["value"], "unit": "samples/s", "samples_per_step": 16384,
@@ -443,7 +483,8 @@ def run_chain(args, rank, world, local_rank, emit=True):
     torch.cuda.set_device(device)
     if world > 1 and not dist.is_initialized():
         dist.init_process_group("nccl", device_id=device)
-    cs = pkg.ChainSampler(inst.g, inst.u, inst.order, device=device, precision="c64", batch_tile=args.tile64)
+    chain_tile = args.tile64 or 128
+    cs = pkg.ChainSampler(inst.g, inst.u, inst.order, device=device, precision="c64", batch_tile=chain_tile)
     stream = torch.cuda.current_stream(device)
     outs = cs._outs(BATCH)
     seed = [1000 + rank]
@@ -481,11 +522,11 @@ def run_chain(args, rank, world, local_rank, emit=True):
             "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded graph and gates, Philox uniforms)",
             "config": {"workload": f"n=40 random 3-regular, r_max {inst.rmax}, {BATCH} samples per GPU per step",
-                       "instance": inst.name, "batch_tile": args.tile64},
+                       "instance": inst.name, "batch_tile": chain_tile},
             "roofline": {"bound": "hbm", "achieved": bytes_per * BATCH * args.steps / t / 1e9,
                          "algorithmic_bytes_per_step": bytes_per * BATCH},
             "checks": {"max_abs_logp_minus_log_p": consistency, "linear_xeb": xeb},
-            "gpu_launches": args.steps * -(-BATCH // args.tile64) * (3 * N_QUBITS + 3),
+            "gpu_launches": args.steps * -(-BATCH // chain_tile) * (3 * N_QUBITS + 3),
             "clocks": clocks.summary()}
     if emit and rank == 0:
         print(json.dumps(line), flush=True)
@@ -500,8 +541,10 @@ BATCH_SEED = 2026
 
 def batched_instances(pkg, count, max_rank):
     """Uneven instances: n uniform in [20, 36], Erdos-Renyi graphs of average degree 3,
-    Haar SU(2) gates; order = the lowest max rank among 64 seeded random orders (2048
-    when that is above the resident maximum)."""
+    Haar SU(2) gates.  Order: the lowest max rank among 64 seeded random orders (2048 when
+    that is above the resident maximum), then 20,000 steps of the package's order search
+    (seeded; one host thread per instance)."""
+    from concurrent.futures import ThreadPoolExecutor
     rng = np.random.default_rng(BATCH_SEED)
     out = []
     for i in range(count):
@@ -512,7 +555,13 @@ def batched_instances(pkg, count, max_rank):
             inst = pkg.instances.make_instance("er3", n, 300000 + i, pkg.rank_profile, target_rank=0,
                                                order_seeds=range(2048))
         out.append(inst)
-    return out
+
+    def search(inst):
+        order, ranks, _ = pkg.search_order(inst.n, pkg.edges_from_graph(inst.g), inst.order, iterations=20000,
+                                           seed=1, threads=1)
+        return pkg.instances.Instance(inst.g, inst.u, order, ranks, inst.name + "-searched")
+    with ThreadPoolExecutor(max(1, min(16, host_cores()))) as ex:
+        return list(ex.map(search, out))
 
 
 def run_batched(args, rank, world, local_rank):
@@ -610,7 +659,7 @@ def run_batched(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64",
             "data": "synthetic (seeded graphs, gates, strings; Philox uniforms)",
-            "config": {"workload": f"{nI} Erdos-Renyi instances (avg degree 3, n in [20,36], r_max "
+            "config": {"workload": f"{nI} Erdos-Renyi instances (avg degree 3, n in [20,36], searched orders, r_max "
                                    f"{min(i.rmax for i in insts)}-{max(i.rmax for i in insts)}): {K} amplitudes + "
                                    f"{S} samples each per step, one persistent launch replayed from a CUDA graph",
                        "instances": nI, "strings_per_instance": K, "samples_per_instance": S,
@@ -856,7 +905,10 @@ def main():
     ap.add_argument("--samples", type=int, default=4096, help="accepted samples of the learned workload")
     ap.add_argument("--epochs", type=int, default=8, help="training epochs of the learned workload")
     ap.add_argument("--m", type=int, default=30, help="conditional qubits of the fourier workload")
-    ap.add_argument("--tile64", type=int, default=128)
+    ap.add_argument("--tile64", type=int, default=None, help="complex64 batch tile (default: 256 c64f32, 128 c64)")
+    ap.add_argument("--bulk", choices=["c64f32", "c64"], default="c64f32",
+                    help="complex64 bulk arithmetic: float32 (default) or float64")
+    ap.add_argument("--no-alt", action="store_true", help="skip timing the other complex64 recipe")
     ap.add_argument("--tile128", type=int, default=64)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))

@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <mutex>
 
 #include "common.hpp"
@@ -44,7 +45,7 @@ FourierPlan::~FourierPlan() {
   int prev = -1;
   cudaGetDevice(&prev);
   cudaSetDevice(device);
-  for (void* p : {d_lut_z, d_lut_a, d_lut_cols, d_uA, d_uB})
+  for (void* p : {d_lut_z, d_lut_a, d_lut_cols, d_uA, d_uB, d_rot, d_dg, d_dh, d_rg, d_rh})
     if (p) cudaFree(p);
   if (prev >= 0) cudaSetDevice(prev);
 }
@@ -67,6 +68,12 @@ struct PassParams {
   const double2* wspec;           // [(m+1)^2] popcount weights
   u64 outmask;
   const double2* u;               // [m][2][2] complex128 per global bit
+  const float2* rot;              // [m] (c, s): products are real rotations (Euler-factorised path)
+  const float2* dg;               // chunk tables of the diagonal applied with the q_A phase, or null
+  const float2* dh;               // chunk tables of the diagonal applied after the products, or null
+  const float2* rg;               // [m] per-bit ratios d_j(1) / d_j(0) of the dg diagonal
+  const float2* rh;               // [m] per-bit ratios of the dh diagonal
+  const float2* wspecf;           // [(m+1)^2] popcount weights as complex64
   double* masses;                 // per tile or null
   int store;
 };
@@ -134,6 +141,44 @@ __device__ __forceinline__ void tile_lut_eval(const u64* lut, const TileLut& t, 
   pm &= z | (1ull << 63);
 }
 
+// Phase-parity mask of z alone (the q_A phase needs no map part).
+__device__ __forceinline__ u64 tile_lut_pm(const u64* lut, const TileLut& t, u64 z) {
+  u64 pm = t.pm_const;
+  for (int cc = 0; cc < t.chunks; ++cc) {
+    if (!((t.var >> cc) & 1u)) continue;
+    pm ^= __ldg(lut + ((((u64)cc << 8) + ((z >> (8 * cc)) & 255ull)) << 1) + 1);
+  }
+  return pm & (z | (1ull << 63));
+}
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+
+// A diagonal D(z) = prod_j d_j(z_j) over the state index, applied inside a tile: with the
+// tile's varying bits zero in `base`, D(base ^ f) = D(base) prod_{a: f_a = 1} r_a for the
+// tile-local bits a (r_a = d(1) / d(0) of that bit).  Three 16-entry window tables
+// (tile-local bits 0-3, 4-7, 8-11; D(base) folded into the first) make the factor of
+// element f two complex products.  D(base) comes from the 8-bit chunk tables T.
+__device__ __forceinline__ void window_tables(float2 (*wt)[16], const PassParams& P, const float2* T,
+                                              const float2* ratio, u64 base, int TB) {
+  for (int t = threadIdx.x; t < 48; t += blockDim.x) {
+    const int w = t >> 4, i = t & 15;
+    float2 v = make_float2(1.f, 0.f);
+    if (w == 0)
+      for (int cc = 0; cc < P.chunks; ++cc) v = cmulf(v, __ldg(T + ((u64)cc << 8) + ((base >> (8 * cc)) & 255ull)));
+    for (int a = 0; a < 4; ++a) {
+      const int la = 4 * w + a;
+      if (la < TB && ((i >> a) & 1)) v = cmulf(v, __ldg(ratio + local_to_global_bit(P, la)));
+    }
+    wt[w][i] = v;
+  }
+}
+
+__device__ __forceinline__ float2 window_factor(const float2 (*wt)[16], int f) {
+  return cmulf(cmulf(wt[0][f & 15], wt[1][(f >> 4) & 15]), wt[2][(f >> 8) & 15]);
+}
+
 // Initial value at index z (fourier_covariant_sampler.py:78-86, init_specialization.py:196-214,
 // distributed_sampler.py:14-20).  For INIT_PRODUCT the table has no map part (b = z).
 __device__ float2 init_value(const PassParams& P, const TileLut& t, u64 z) {
@@ -142,7 +187,9 @@ __device__ float2 init_value(const PassParams& P, const TileLut& t, u64 z) {
   if (P.init == INIT_PRODUCT) b = z;
   double2 w;
   if (P.init == INIT_COV_SPECIAL) {
-    w = __ldg(P.wspec + __popcll(b) * (P.m + 1) + __popcll(b & P.outmask));
+    const float2 wf = __ldg(P.wspecf + __popcll(b) * (P.m + 1) + __popcll(b & P.outmask));
+    const float s = (__popcll(pm) & 1) ? -1.f : 1.f;
+    return make_float2(s * wf.x, s * wf.y);
   } else {
     w = __ldg(P.wgen + ((b & 255ull)));
     for (int cc = 1; cc < P.chunks; ++cc) w = cmul(w, __ldg(P.wgen + ((u64)cc << 8) + ((b >> (8 * cc)) & 255ull)));
@@ -156,6 +203,14 @@ __device__ __forceinline__ void apply_u(float2& x, float2& y, const float2 (&u)[
                                 u[0].x * x.y + u[0].y * x.x + u[1].x * y.y + u[1].y * y.x);
   const float2 ny = make_float2(u[2].x * x.x - u[2].y * x.y + u[3].x * y.x - u[3].y * y.y,
                                 u[2].x * x.y + u[2].y * x.x + u[3].x * y.y + u[3].y * y.x);
+  x = nx;
+  y = ny;
+}
+
+// Real rotation [[c, -s], [s, c]] on a pair of complex values: 4 FMUL + 4 FFMA.
+__device__ __forceinline__ void apply_rot(float2& x, float2& y, float c, float s) {
+  const float2 nx = make_float2(fmaf(c, x.x, -s * y.x), fmaf(c, x.y, -s * y.y));
+  const float2 ny = make_float2(fmaf(s, x.x, c * y.x), fmaf(s, x.y, c * y.y));
   x = nx;
   y = ny;
 }
@@ -182,6 +237,13 @@ __device__ void tile_round(float2* sm, const PassParams& P, int w0, unsigned mas
         const float2 x = r[i], y = r[i | (1 << a)];
         r[i] = make_float2(x.x + y.x, x.y + y.y);
         r[i | (1 << a)] = make_float2(x.x - y.x, x.y - y.y);
+      }
+    } else if (P.rot) {
+      const float2 cs = __ldg(P.rot + local_to_global_bit(P, w0 + a));
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        if (i & (1 << a)) continue;
+        apply_rot(r[i], r[i | (1 << a)], cs.x, cs.y);
       }
     } else {
       const double2* u4 = P.u + 4 * local_to_global_bit(P, w0 + a);
@@ -222,6 +284,7 @@ __device__ void tile_rounds(float2* sm, const PassParams& P, int TB, unsigned ma
 
 __global__ void __launch_bounds__(256, 3) fourier_pass_kernel(const __grid_constant__ PassParams P) {
   extern __shared__ float2 sm[];
+  __shared__ float2 wt[3][16];  // window tables of a diagonal (see window_tables)
   const int TB = P.c + P.K;
   const int nt = 1 << (TB - 4);
   const u64 tile = blockIdx.x;
@@ -258,37 +321,47 @@ __global__ void __launch_bounds__(256, 3) fourier_pass_kernel(const __grid_const
   }
   if (P.wht_mask) tile_rounds(sm, P, TB, P.wht_mask, true);
   if (P.phase) {
+    // q_A phase (-1)^{q_A(z)}, times the diagonal dg when given.
     TileLut t;
     tile_lut(P.lut_a, P.chunks, base, varying, t);
+    if (P.dg) window_tables(wt, P, P.dg, P.rg, base, TB);
     __syncthreads();
     for (int k = 0; k < 8; ++k) {
       const int f = 2 * (threadIdx.x + k * nt);
       const u64 g = tile_global(P, tile, f);
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
-        u64 b, pm;
-        tile_lut_eval(P.lut_a, t, g + e, b, pm);
-        if (__popcll(pm) & 1) {
-          const float2 x = sm[pad(f + e)];
-          sm[pad(f + e)] = make_float2(-x.x, -x.y);
-        }
+        float2 x = sm[pad(f + e)];
+        if (P.dg) x = cmulf(x, window_factor(wt, f + e));
+        if (__popcll(tile_lut_pm(P.lut_a, t, g + e)) & 1) x = make_float2(-x.x, -x.y);
+        sm[pad(f + e)] = x;
       }
     }
   }
   if (P.u_mask) tile_rounds(sm, P, TB, P.u_mask, false);
+  if (P.dh) {
+    __syncthreads();  // the phase loop's readers of wt are done
+    window_tables(wt, P, P.dh, P.rh, base, TB);
+  }
   __syncthreads();
-  double mass = 0.0;
+  float mass = 0.f;  // 16 elements per thread: float partial, then float64 across threads
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const int f = 2 * (threadIdx.x + k * nt);
-    const float2 a = sm[pad(f)], b = sm[pad(f + 1)];
-    if (P.store) *reinterpret_cast<float4*>(P.v + tile_global(P, tile, f)) = make_float4(a.x, a.y, b.x, b.y);
-    if (P.masses) mass += (double)a.x * a.x + (double)a.y * a.y + (double)b.x * b.x + (double)b.y * b.y;
+    const u64 g = tile_global(P, tile, f);
+    float2 a = sm[pad(f)], b = sm[pad(f + 1)];
+    if (P.dh) {
+      a = cmulf(a, window_factor(wt, f));
+      b = cmulf(b, window_factor(wt, f + 1));
+    }
+    if (P.store) *reinterpret_cast<float4*>(P.v + g) = make_float4(a.x, a.y, b.x, b.y);
+    if (P.masses) mass = fmaf(a.x, a.x, fmaf(a.y, a.y, fmaf(b.x, b.x, fmaf(b.y, b.y, mass))));
   }
   if (P.masses) {
     __shared__ double red[32];
-    for (int off = 16; off; off >>= 1) mass += __shfl_xor_sync(0xffffffffu, mass, off);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mass;
+    double m2 = (double)mass;
+    for (int off = 16; off; off >>= 1) m2 += __shfl_xor_sync(0xffffffffu, m2, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m2;
     __syncthreads();
     if (threadIdx.x == 0) {
       double s = 0.0;
@@ -301,7 +374,8 @@ __global__ void __launch_bounds__(256, 3) fourier_pass_kernel(const __grid_const
 // Per-sample weight tables: generic chunk products over b (with 2^{-m/2} in chunk 0)
 // or the popcount table of identical B unitaries (init_specialization.py:98-115).
 __global__ void fourier_weights_kernel(int m, int chunks, const double2* __restrict__ uB, u64 outmask, int special,
-                                       double2* __restrict__ wgen, double2* __restrict__ wspec, int scale_half_m) {
+                                       double2* __restrict__ wgen, double2* __restrict__ wspec,
+                                       float2* __restrict__ wspecf, int scale_half_m) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   const double scale = scale_half_m ? exp2(-0.5 * m) : 1.0;
   if (!special) {
@@ -327,6 +401,7 @@ __global__ void fourier_weights_kernel(int m, int chunks, const double2* __restr
       }
     }
     wspec[e] = w;
+    wspecf[e] = make_float2((float)w.x, (float)w.y);
   }
 }
 
@@ -599,7 +674,8 @@ int build_weights(FourierPlan& p, uint64_t outB, char* ws, const FourierLayout& 
   double2* w = (double2*)(ws + L.off_weights);
   const int entries = special ? (p.m + 1) * (p.m + 1) : p.chunks * 256;
   fourier_weights_kernel<<<(entries + 255) / 256, 256, 0, s>>>(p.m, p.chunks, (const double2*)p.d_uB, outB,
-                                                               special ? 1 : 0, w, w, scale ? 1 : 0);
+                                                               special ? 1 : 0, w, w, (float2*)(ws + L.off_wspecf),
+                                                               scale ? 1 : 0);
   RGS_CUDA_TRY(cudaGetLastError());
   return RGS_OK;
 }
@@ -613,6 +689,60 @@ int check_state(FourierPlan& p, const void* state, void* ws, size_t ws_bytes, Fo
   int rc = bind_device_of(state, &device);
   if (rc) return rc;
   return fourier_upload(p, device);
+}
+
+// Euler factorisation of a 2x2 unitary: U = diag(h) R diag(g) with R = [[c, -s], [s, c]]
+// (c = cos(beta/2), s = sin(beta/2) >= 0) and unit-modulus h, g -- the ZYZ decomposition
+// with the global phase folded into h.  All products on the A sites then split into one
+// diagonal before (folded into the q_A phase), real rotations (4 FFMA per element and
+// axis instead of 8 for a complex 2x2), and one diagonal after them.  Returns false if
+// the reconstruction misses U by more than 1e-9 (a non-unitary input).
+bool euler_factors(const double* u, std::complex<double> g[2], std::complex<double> h[2], double& c, double& s) {
+  typedef std::complex<double> C;
+  const C a(u[0], u[1]), b(u[2], u[3]), cc(u[4], u[5]), d(u[6], u[7]);
+  c = std::sqrt(0.5 * (std::norm(a) + std::norm(d)));
+  s = std::sqrt(0.5 * (std::norm(b) + std::norm(cc)));
+  const double nrm = std::hypot(c, s);
+  if (!(nrm > 0.0)) return false;
+  c /= nrm;
+  s /= nrm;
+  g[0] = g[1] = C(1.0, 0.0);
+  if (s < 1e-12) {
+    c = 1.0;
+    s = 0.0;
+    h[0] = a / std::abs(a);
+    h[1] = d / std::abs(d);
+  } else if (c < 1e-12) {
+    c = 0.0;
+    s = 1.0;
+    h[0] = -b / std::abs(b);
+    h[1] = cc / std::abs(cc);
+  } else {
+    h[0] = a / std::abs(a);
+    h[1] = cc / std::abs(cc);
+    g[1] = (-b / std::abs(b)) / h[0];
+  }
+  const C r[4] = {h[0] * c * g[0], -h[0] * s * g[1], h[1] * s * g[0], h[1] * c * g[1]};
+  const C v[4] = {a, b, cc, d};
+  double err = 0.0;
+  for (int k = 0; k < 4; ++k) err = std::max(err, std::abs(r[k] - v[k]));
+  return err < 1e-9;
+}
+
+// Chunk tables of a diagonal over m bits: T[c][code] = prod over bits t of chunk c of
+// f_j[bit t of code], j = 8c + t.
+void diag_tables(int m, int chunks, const std::vector<std::complex<double>>& f, std::vector<float>& out) {
+  out.assign((size_t)chunks * 256 * 2, 0.f);
+  for (int cc = 0; cc < chunks; ++cc)
+    for (int code = 0; code < 256; ++code) {
+      std::complex<double> v(1.0, 0.0);
+      for (int t = 0; t < 8; ++t) {
+        const int j = 8 * cc + t;
+        if (j < m) v *= f[2 * j + ((code >> t) & 1)];
+      }
+      out[((size_t)cc * 256 + code) * 2] = (float)v.real();
+      out[((size_t)cc * 256 + code) * 2 + 1] = (float)v.imag();
+    }
 }
 
 }  // namespace
@@ -674,6 +804,38 @@ std::string fourier_build(int n, const uint8_t* graph, const double* unitaries, 
   for (int j = 1; j < m && p.specialized; ++j)
     for (int e = 0; e < 8; ++e)
       if (p.uB[(size_t)j * 8 + e] != p.uB[e]) p.specialized = false;
+  // Euler factors of the A-site unitaries (trivial for the deferred terminal bit).
+  std::vector<std::complex<double>> fg(2 * m, 1.0), fh(2 * m, 1.0);
+  p.rot.assign((size_t)2 * m, 0.f);
+  p.rot_ok = true;
+  for (int j = 0; j < m && p.rot_ok; ++j) {
+    if (deferred && j == m - 1) {
+      p.rot[2 * j] = 1.f;
+      continue;
+    }
+    std::complex<double> g2[2], h2[2];
+    double c = 0.0, sn = 0.0;
+    if (!euler_factors(&p.uA[(size_t)j * 8], g2, h2, c, sn)) p.rot_ok = false;
+    fg[2 * j] = g2[0];
+    fg[2 * j + 1] = g2[1];
+    fh[2 * j] = h2[0];
+    fh[2 * j + 1] = h2[1];
+    p.rot[2 * j] = (float)c;
+    p.rot[2 * j + 1] = (float)sn;
+  }
+  if (p.rot_ok) {
+    diag_tables(m, p.chunks, fg, p.dg);
+    diag_tables(m, p.chunks, fh, p.dh);
+    p.rg.resize((size_t)2 * m);
+    p.rh.resize((size_t)2 * m);
+    for (int j = 0; j < m; ++j) {
+      const std::complex<double> a = fg[2 * j + 1] / fg[2 * j], b = fh[2 * j + 1] / fh[2 * j];
+      p.rg[2 * j] = (float)a.real();
+      p.rg[2 * j + 1] = (float)a.imag();
+      p.rh[2 * j] = (float)b.real();
+      p.rh[2 * j + 1] = (float)b.imag();
+    }
+  }
   p.ngroups = (int)strided_groups(m).size();
   status = RGS_OK;
   return "";
@@ -685,7 +847,8 @@ void fourier_layout(const FourierPlan& p, FourierLayout& L) {
   L.off_masses = 0;
   L.off_weights = align_up((size_t)L.ntiles * sizeof(double), 256);
   const size_t wentries = std::max<size_t>((size_t)p.chunks * 256, (size_t)(p.m + 1) * (p.m + 1));
-  L.off_result = L.off_weights + align_up(wentries * 16, 256);
+  L.off_wspecf = L.off_weights + align_up(wentries * 16, 256);
+  L.off_result = L.off_wspecf + align_up((size_t)(p.m + 1) * (p.m + 1) * 8, 256);
   L.total = L.off_result + 256;
 }
 
@@ -710,6 +873,13 @@ int fourier_upload(FourierPlan& p, int device) {
   if ((rc = up(&p.d_lut_cols, p.lut_cols.data(), p.lut_cols.size() * 8))) return rc;
   if ((rc = up(&p.d_uA, p.uA.data(), p.uA.size() * 8))) return rc;
   if ((rc = up(&p.d_uB, p.uB.data(), p.uB.size() * 8))) return rc;
+  if (p.rot_ok) {
+    if ((rc = up(&p.d_rot, p.rot.data(), p.rot.size() * 4))) return rc;
+    if ((rc = up(&p.d_dg, p.dg.data(), p.dg.size() * 4))) return rc;
+    if ((rc = up(&p.d_dh, p.dh.data(), p.dh.size() * 4))) return rc;
+    if ((rc = up(&p.d_rg, p.rg.data(), p.rg.size() * 4))) return rc;
+    if ((rc = up(&p.d_rh, p.rh.data(), p.rh.size() * 4))) return rc;
+  }
   p.device = device;
   return RGS_OK;
 }
@@ -731,13 +901,23 @@ int fourier_compute(FourierPlan& p, uint64_t outB, void* state, void* ws, size_t
   P.lut_z = (const u64*)p.d_lut_z;
   P.wgen = (const double2*)(w + L.off_weights);
   P.wspec = (const double2*)(w + L.off_weights);
+  P.wspecf = (const float2*)(w + L.off_wspecf);
   P.outmask = outB;
+  P.rg = (const float2*)p.d_rg;
+  P.rh = (const float2*)p.d_rh;
+  // Products as real rotations between the two Euler diagonals: dg with the q_A phase,
+  // dh after the last products.
+  const float2* dg = p.rot_ok ? (const float2*)p.d_dg : nullptr;
+  const float2* dh = p.rot_ok ? (const float2*)p.d_dh : nullptr;
+  P.rot = p.rot_ok ? (const float2*)p.d_rot : nullptr;
   double* masses = (double*)(w + L.off_masses);
   const int m = p.m;
   if (m <= kTileBits) {
     contiguous(P, m);
     P.wht_mask = (1u << m) - 1u;
     P.phase = 1;
+    P.dg = dg;
+    P.dh = dh;
     P.u_mask = product_mask(p, P, (1u << m) - 1u);
     P.masses = masses;
     if ((rc = launch_pass(P, s))) return rc;
@@ -761,10 +941,12 @@ int fourier_compute(FourierPlan& p, uint64_t outB, void* state, void* ws, size_t
     strided(P, groups[k - 1].first, groups[k - 1].second);
     P.wht_mask = target_mask(P);
     P.phase = 1;
+    P.dg = dg;
     P.u_mask = product_mask(p, P, target_mask(P));
     if ((rc = launch_pass(P, s))) return rc;
     if (stages) RGS_CUDA_TRY(cudaEventRecord(ev[2], s));
     P.phase = 0;
+    P.dg = nullptr;
     P.wht_mask = 0;
     for (int i = k - 2; i >= 0; --i) {
       strided(P, groups[i].first, groups[i].second);
@@ -773,6 +955,7 @@ int fourier_compute(FourierPlan& p, uint64_t outB, void* state, void* ws, size_t
     }
     contiguous(P, m);
     P.u_mask = product_mask(p, P, (1u << kTileBits) - 1u);
+    P.dh = dh;
     P.masses = masses;
     if ((rc = launch_pass(P, s))) return rc;
   }

@@ -27,6 +27,14 @@ struct FourierPlan {
   std::vector<u64h> qB, qA;      // strict-upper masks of g_BB, g_AA (distributed_sampler.py:57)
   std::vector<u64h> cols;        // cols[k] = mask over B of g[A_k, B] (distributed_sampler.py:68)
   std::vector<double> uA, uB;    // complex128 [m][2][2] of the A / B sites
+  // Euler factors of the A-site unitaries, U_j = diag(h_j) R(c_j, s_j) diag(g_j) with R a
+  // real rotation (see fourier.cu): per-bit rotations and 8-bit-chunk tables of the two
+  // diagonals (the deferred terminal bit has trivial factors).  rot_ok = false falls
+  // back to general 2x2 products (a non-unitary input).
+  bool rot_ok = false;
+  std::vector<float> rot;        // [m][2] (c, s)
+  std::vector<float> dg, dh;     // [chunks][256][2] complex64 chunk products of g / h
+  std::vector<float> rg, rh;     // [m][2] per-bit ratios g(1)/g(0), h(1)/h(0)
   // Pass schedule (see fourier.cu).
   int ngroups = 0;               // strided target groups above the low tile
   // Device copies.
@@ -36,12 +44,17 @@ struct FourierPlan {
   void* d_lut_cols = nullptr;
   void* d_uA = nullptr;          // complex64 [m][2][2]
   void* d_uB = nullptr;          // complex128 [m][2][2]
+  void* d_rot = nullptr;         // float2 [m]
+  void* d_dg = nullptr;          // float2 [chunks][256]
+  void* d_dh = nullptr;          // float2 [chunks][256]
+  void* d_rg = nullptr;          // float2 [m]
+  void* d_rh = nullptr;          // float2 [m]
   ~FourierPlan();
 };
 
 // Workspace: per-tile masses (double), per-sample weight tables, draw result.
 struct FourierLayout {
-  size_t off_masses = 0, off_weights = 0, off_result = 0, total = 0;
+  size_t off_masses = 0, off_weights = 0, off_wspecf = 0, off_result = 0, total = 0;
   long long ntiles = 0;
 };
 

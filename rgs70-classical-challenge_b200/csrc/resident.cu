@@ -175,17 +175,40 @@ __device__ __forceinline__ void row_gram(const typename Pair2<S>::T* __restrict_
   }
 }
 
+// The item's maximum |E|^2 of the last step (over the threads that own its rows), with
+// the zero / non-finite bookkeeping of scan_finalize_kernel.
+template <typename S>
+__device__ __forceinline__ void fold_max(const u64* redm, int tid, int lnb, int slots, ItemState& s) {
+  u64 m = 0;
+  for (int k = 0; k < slots; ++k) {
+    const u64 x = redm[tid + (k << lnb)];
+    m = m > x ? m : x;
+  }
+  const double m2 = max_value<S>(m);
+  if (!s.done) {
+    if (!isfinite(m2))
+      s.done = 2;
+    else if (!(m2 > 0.0))
+      s.done = 1;
+  }
+  s.m2 = m2;
+}
+
+// Per position: phase A (all threads: the Gram pass of a sample unit; item threads: the
+// previous position's maximum, then the weights of an amplitude unit; thread 0: the next
+// step record), a barrier, [sample units: decision and weights, a barrier], the step
+// (rows of the chosen branch, per-thread maxima), a barrier.
 template <typename S, typename M>
 __global__ void __launch_bounds__(kResThreads, 1)
     resident_kernel(const ResInstance* __restrict__ insts, const ResWork* __restrict__ work, long long nwork,
                     int* __restrict__ counter) {
   typedef typename Pair2<S>::T V;
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ double red[kResThreads][4];
+  __shared__ double red[4][kResThreads];  // Gram partials, structure of arrays (no bank conflicts)
   __shared__ u64 redm[kResThreads];
   __shared__ Cx<M> wA[kMaxResItems], wB[kMaxResItems];
   __shared__ ItemState ist[kMaxResItems];
-  __shared__ DevStep sst;
+  __shared__ DevStep sst[2];
   __shared__ long long s_unit;
   const int tid = threadIdx.x;
   const size_t cap = (size_t)kResidentSmem / (2 * sizeof(V));
@@ -218,45 +241,78 @@ __global__ void __launch_bounds__(kResThreads, 1)
       }
       ist[tid] = s;
     }
+    if (tid == 0) sst[0] = in.steps[0];
+    __syncthreads();
     int cur = 0;
     for (int j = 0; j < in.n; ++j) {
-      __syncthreads();  // the previous position's readers of sst, ist and the weights are done
-      if (tid == 0) sst = in.steps[j];
-      __syncthreads();
-      const int mode = sst.mode, v = sst.v;
-      const u64* T = in.tables + sst.table_off;
+      const DevStep& st = sst[j & 1];
+      const int mode = st.mode, v = st.v;
+      const u64* T = in.tables + st.table_off;
       const V* Ein = bufs[cur];
       V* Eout = bufs[cur ^ 1];
       const bool unit = j == 0;
-      const u64 rows = mode == MODE_PAIR ? (1ull << (sst.r_out - 1)) : (1ull << sst.r_out);
+      const u64 rows = mode == MODE_PAIR ? (1ull << (st.r_out - 1)) : (1ull << st.r_out);
+      const bool analytic = mode == MODE_PAIR && st.ncombos == 1;
+
+      // ---- phase A
+      if (sample && !analytic) {
+        // Gram matrix of this position from the table (chain_gram_kernel's accumulation).
+        double g0 = 0.0, g1 = 0.0, g2 = 0.0, g3 = 0.0;
+        for (u64 r = slot; r < rows; r += slots) {
+          const u64 ca = mode == MODE_PAIR ? deposit_zero(r, st.pi) : r;
+          row_gram<S>(Ein, st, table_lookup(T, st.nbytes, ca), lnb, b, unit, g0, g1, g2, g3);
+        }
+        red[0][tid] = g0;
+        red[1][tid] = g1;
+        red[2][tid] = g2;
+        red[3][tid] = g3;
+      }
+      if (tid < nb) {
+        ItemState& s = ist[tid];
+        if (j > 0) fold_max<S>(redm, tid, lnb, slots, s);
+        if (!sample) {
+          // Weights of the given bit (scan_weights_kernel), with the fixed-vertex offsets.
+          const DevVert vt = in.verts[j];
+          const double sc = ldexp(1.0, -scale_exponent(s.m2));
+          const int x = (int)((v < 64 ? (s.lo >> v) : (s.hi >> (v - 64))) & 1ull);
+          const double2 f0 = U2[(v * 2 + x) * 2 + 0], f1 = U2[(v * 2 + x) * 2 + 1];
+          const int ov = (int)((j < 64 ? (s.olo >> j) : (s.ohi >> (j - 64))) & 1ull);
+          if (j < 64)
+            s.olo &= ~(1ull << j);
+          else
+            s.ohi &= ~(1ull << (j - 64));
+          int y = 0;
+          if (vt.fixed) {
+            y = hypot(f0.x, f0.y) > 1e-12 ? 0 : 1;
+            if (y) {
+              s.olo ^= vt.fut_lo;
+              s.ohi ^= vt.fut_hi;
+            }
+          }
+          Cx<M> wa, wb;
+          branch_weights<M>(f0, f1, sc, mode, y, wa, wb);
+          if (tid >= wk.num) wa = wb = Cx<M>{(M)0, (M)0};
+          wA[tid] = wa;
+          wB[tid] = wb;
+          s.flags = y | (ov << 1);
+          if (!s.done) s.esum += scale_exponent(s.m2);
+        }
+      }
+      if (tid == 0 && j + 1 < in.n) sst[(j + 1) & 1] = in.steps[j + 1];
+      __syncthreads();
 
       if (sample) {
-        // Both branch masses from the position's Gram matrix (chain_gram_kernel), or in
-        // closed form on a one-combo pair position; then the decision (chain_decide_kernel).
-        const bool analytic = mode == MODE_PAIR && sst.ncombos == 1;
-        if (!analytic) {
-          double g0 = 0.0, g1 = 0.0, g2 = 0.0, g3 = 0.0;
-          for (u64 r = slot; r < rows; r += slots) {
-            const u64 ca = mode == MODE_PAIR ? deposit_zero(r, sst.pi) : r;
-            const u64 p0 = table_lookup(T, sst.nbytes, ca);
-            row_gram<S>(Ein, sst, p0, lnb, b, unit, g0, g1, g2, g3);
-          }
-          red[tid][0] = g0;
-          red[tid][1] = g1;
-          red[tid][2] = g2;
-          red[tid][3] = g3;
-        }
-        __syncthreads();
+        // Both branch masses (or their closed form), the decision (chain_decide_kernel).
         if (tid < nb) {
           double g0 = 1.0, g1 = 1.0, g2 = 0.0, g3 = 0.0;
           if (!analytic) {
             g0 = g1 = 0.0;
             for (int k = 0; k < slots; ++k) {
-              const double* q = red[tid + (k << lnb)];
-              g0 += q[0];
-              g1 += q[1];
-              g2 += q[2];
-              g3 += q[3];
+              const int q = tid + (k << lnb);
+              g0 += red[0][q];
+              g1 += red[1][q];
+              g2 += red[2][q];
+              g3 += red[3][q];
             }
           }
           const double m0 = branch_mass(U2 + (v * 2 + 0) * 2, g0, g1, g2, g3);
@@ -280,84 +336,45 @@ __global__ void __launch_bounds__(kResThreads, 1)
             }
           }
           const double sc = ldexp(1.0, -scale_exponent(s.m2));
-          Cx<M> a, c;
-          branch_weights<M>(U2[(v * 2 + x) * 2 + 0], U2[(v * 2 + x) * 2 + 1], sc, mode, 0, a, c);
-          if (tid >= wk.num) a = c = Cx<M>{(M)0, (M)0};
-          wA[tid] = a;
-          wB[tid] = c;
+          Cx<M> wa, wb;
+          branch_weights<M>(U2[(v * 2 + x) * 2 + 0], U2[(v * 2 + x) * 2 + 1], sc, mode, 0, wa, wb);
+          if (tid >= wk.num) wa = wb = Cx<M>{(M)0, (M)0};
+          wA[tid] = wa;
+          wB[tid] = wb;
           s.flags = 0;
           if (!s.done) s.esum += scale_exponent(s.m2);
         }
-      } else if (tid < nb) {
-        // Weights of the given bit (scan_weights_kernel), with the fixed-vertex offsets.
-        ItemState& s = ist[tid];
-        const DevVert vt = in.verts[j];
-        const double sc = ldexp(1.0, -scale_exponent(s.m2));
-        const int x = (int)((v < 64 ? (s.lo >> v) : (s.hi >> (v - 64))) & 1ull);
-        const double2 f0 = U2[(v * 2 + x) * 2 + 0], f1 = U2[(v * 2 + x) * 2 + 1];
-        const int ov = (int)((j < 64 ? (s.olo >> j) : (s.ohi >> (j - 64))) & 1ull);
-        if (j < 64)
-          s.olo &= ~(1ull << j);
-        else
-          s.ohi &= ~(1ull << (j - 64));
-        int y = 0;
-        if (vt.fixed) {
-          y = hypot(f0.x, f0.y) > 1e-12 ? 0 : 1;
-          if (y) {
-            s.olo ^= vt.fut_lo;
-            s.ohi ^= vt.fut_hi;
-          }
-        }
-        Cx<M> a, c;
-        branch_weights<M>(f0, f1, sc, mode, y, a, c);
-        if (tid >= wk.num) a = c = Cx<M>{(M)0, (M)0};
-        wA[tid] = a;
-        wB[tid] = c;
-        s.flags = y | (ov << 1);
-        if (!s.done) s.esum += scale_exponent(s.m2);
+        __syncthreads();
       }
-      __syncthreads();
 
-      // The step: rows c' (and c'^t) of the chosen branch, per-item maximum of |E|^2.
+      // ---- the step: rows c' (and c'^t) of the chosen branch, per-thread maxima.
       {
         const Cx<M> wa = wA[b], wb = wB[b];
         const int fl = ist[b].flags;
         S mx = (S)0;
+#pragma unroll 2
         for (u64 r = slot; r < rows; r += slots) {
-          const u64 ca = mode == MODE_PAIR ? deposit_zero(r, sst.pi) : r;
-          const u64 p0 = table_lookup(T, sst.nbytes, ca);
+          const u64 ca = mode == MODE_PAIR ? deposit_zero(r, st.pi) : r;
           Cx<M> oa, ob;
-          row_outputs<S, M>(Ein, sst, p0, lnb, b, unit, wa, wb, (fl >> 1) & 1, fl & 1, oa, ob);
+          row_outputs<S, M>(Ein, st, table_lookup(T, st.nbytes, ca), lnb, b, unit, wa, wb, (fl >> 1) & 1, fl & 1,
+                            oa, ob);
           const S ar = (S)oa.re, ai = (S)oa.im;
           Eout[(ca << lnb) + b] = V{ar, ai};
           mx = fmax(mx, norm2(ar, ai));
           if (mode == MODE_PAIR) {
             const S br = (S)ob.re, bi = (S)ob.im;
-            Eout[((ca ^ sst.t) << lnb) + b] = V{br, bi};
+            Eout[((ca ^ st.t) << lnb) + b] = V{br, bi};
             mx = fmax(mx, norm2(br, bi));
           }
         }
         redm[tid] = max_bits<S>(mx);
       }
-      __syncthreads();
-      if (tid < nb) {
-        u64 m = 0;
-        for (int k = 0; k < slots; ++k) m = m > redm[tid + (k << lnb)] ? m : redm[tid + (k << lnb)];
-        const double m2 = max_value<S>(m);
-        ItemState& s = ist[tid];
-        if (!s.done) {
-          if (!isfinite(m2))
-            s.done = 2;
-          else if (!(m2 > 0.0))
-            s.done = 1;
-        }
-        s.m2 = m2;
-      }
       cur ^= 1;
+      __syncthreads();
     }
-    __syncthreads();
     if (tid < wk.num) {
-      const ItemState s = ist[tid];
+      ItemState s = ist[tid];
+      fold_max<S>(redm, tid, lnb, slots, s);
       const V e = bufs[cur][tid];  // row 0 of the final table
       S re = e.x, im = e.y;
       if (s.done == 1) re = im = (S)0;
@@ -375,7 +392,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
         in.out_logscale[item] = ls;
       }
     }
-    // The next iteration's first barrier orders these reads before s_unit is rewritten.
+    // The next unit's first barrier orders these reads before ist and s_unit are rewritten.
   }
 }
 

@@ -19,7 +19,7 @@ import torch
 from . import _lib
 from .plan import ScanPlan, edges_from_graph
 
-__all__ = ["ScanEngine", "ScanOracle", "pack_bits", "PRECISIONS", "max_batch_tile"]
+__all__ = ["ScanEngine", "ScanOracle", "pack_bits", "PRECISIONS", "max_batch_tile", "capture_graph"]
 
 PRECISIONS = {"c64": _lib.PREC_C64, "c64f32": _lib.PREC_C64_F32, "c128": _lib.PREC_C128}
 LN2 = math.log(2.0)
@@ -39,6 +39,23 @@ def pack_bits(bits, n=None):
     padded = np.zeros((b.shape[0], 128), dtype=np.uint8)
     padded[:, :b.shape[1]] = b
     return np.ascontiguousarray(np.packbits(padded, axis=1, bitorder="little").view("<u8"))
+
+
+def capture_graph(device, fn):
+    """Capture ``fn(stream)`` -- queued library calls on ``stream`` -- into a CUDA graph;
+    replay it with ``graph.replay()`` on the current stream.  Workspaces and outputs must
+    already exist (a capture allocates nothing); run ``fn`` once eagerly first."""
+    device = torch.device(device) if not isinstance(device, torch.device) else device
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.device(device):
+        s = torch.cuda.Stream(device)
+        s.wait_stream(torch.cuda.current_stream(device))
+        with torch.cuda.stream(s):
+            g.capture_begin()
+            fn(s)
+            g.capture_end()
+        torch.cuda.current_stream(device).wait_stream(s)
+    return g
 
 
 def max_batch_tile(precision):
