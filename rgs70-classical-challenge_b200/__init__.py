@@ -14,6 +14,7 @@ from .samplers import ConditionalSampler, DrawRecorder, produce, fwht, product, 
 from .chain import ChainSampler, unpack_bits
 from .batch import ResidentBatch
 from . import batch
+from . import frontend
 from . import proposal
 from .proposal import MadeProposal, rejection_sample, capped_rejection, calibrate_envelope
 
