@@ -803,6 +803,82 @@ def run_rgs70(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def run_full(args, rank, world, local_rank):
+    """Full scale on one GPU: n = 70 random degree-<=3 graph, Haar SU(2) gates, the seeded
+    random order whose max rank is closest to 30 (two complex64 2^30 tables per sample);
+    `--samples` exact Born samples by the chain rule (complex64 tables, float64 branch
+    masses), 256 of them rescored in complex128, linear XEB with the rescored p.  Then the
+    same instance with the order from the package's order search."""
+    import torch
+    import __graft_entry__
+    pkg = __graft_entry__.package()
+    device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+    inst = pkg.instances.make_instance("deg3", 70, 70, pkg.rank_profile, target_rank=30,
+                                       order_seeds=range(1000, 1256))
+    edges = pkg.edges_from_graph(inst.g)
+    searched, _, _ = pkg.search_order(70, edges, inst.order, iterations=200000, seed=1,
+                                      threads=max(1, min(16, host_cores())))
+    stream = torch.cuda.current_stream(device)
+    S = args.samples
+    legs = {}
+    with ClockSampler(local_rank) as clocks:
+        for name, order in (("random_order", inst.order), ("searched_order", searched)):
+            plan = pkg.ScanPlan(70, edges, order)
+            tile = 1
+            while tile < 128 and 2 * (2 * tile) * 8 * (1 << plan.rmax) <= 120 * 2 ** 30:
+                tile *= 2
+            cs = pkg.ChainSampler(inst.g, inst.u, order, device=device, precision="c64", batch_tile=tile, plan=plan)
+            cs.sample_device(min(S, tile), seed=1, check=True, stream=stream)  # warm-up
+            outs = cs._outs(S)
+            torch.cuda.synchronize(device)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            bits, value, logscale, logp = cs.sample_device(S, seed=7000 + rank, check=False, stream=stream, outs=outs)
+            e1.record(stream)
+            torch.cuda.synchronize(device)
+            t = e0.elapsed_time(e1) / 1e3
+            samples = pkg.unpack_bits(bits.cpu().numpy(), 70)
+            p64 = np.abs(pkg.amplitudes_from(value.cpu().numpy().astype(np.complex128), logscale.cpu().numpy(),
+                                             70)) ** 2
+            lp = logp.cpu().numpy()
+            legs[name] = {"samples_per_s": S / t, "seconds": t, "rmax": plan.rmax, "sum_states": plan.sum_states,
+                          "batch_tile": tile, "achieved_GBps": chain_bytes(plan, 8) * S / t / 1e9,
+                          "samples": samples, "p64": p64, "logp": lp}
+            del cs, outs, bits, value, logscale, logp
+            torch.cuda.synchronize(device)
+            torch.cuda.empty_cache()
+    # complex128 rescoring of 256 samples of each leg with the searched order (any order
+    # gives the same p(x); the searched one is cheap).
+    so = pkg.ScanOracle(inst.g, inst.u, searched, device=device, fp64=True)
+    out = {}
+    for name, leg in legs.items():
+        k = min(256, S)
+        p128 = so.probabilities(leg["samples"][:k])
+        rel = np.abs(leg["p64"][:k] - p128) / p128
+        out[name] = {key: leg[key] for key in ("samples_per_s", "seconds", "rmax", "sum_states", "batch_tile",
+                                               "achieved_GBps")}
+        out[name].update({"rescored": k, "max_rel_err_c64_vs_c128": float(rel.max()),
+                          "max_abs_logp_minus_log_p128": float(np.max(np.abs(leg["logp"][:k] - np.log(p128)))),
+                          "linear_xeb_rescored": float((2.0 ** 70) * p128.mean() - 1),
+                          "linear_xeb_all_c64": float((2.0 ** 70) * leg["p64"].mean() - 1)})
+    peaks_path = ROOT / "MEASURED_PEAKS.json"
+    peak = float(json.loads(peaks_path.read_text())["hbm_gbs"]) if peaks_path.exists() else 6650.0
+    main = out["random_order"]
+    line = {"metric": "exact_born_samples_per_s (n=70 degree<=3, rank 30, chain rule, complex64)",
+            "value": main["samples_per_s"], "unit": "samples/s", "n_gpus": world, "steps": 1, "warmup": 1,
+            "ms_per_step": 1e3 * main["seconds"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64", "data": "synthetic (seeded graph, gates, Philox uniforms)",
+            "config": {"workload": f"full scale: n=70 random degree<=3 graph, seeded random order with r_max "
+                                   f"{main['rmax']}, {S} exact samples, 256 rescored in complex128",
+                       "instance": inst.name},
+            "roofline": {"bound": "hbm", "achieved": main["achieved_GBps"], "peak": peak, "unit": "GB/s",
+                         "frac": main["achieved_GBps"] / peak, "traffic": None},
+            "legs": out, "clocks": clocks.summary()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_learned(args, rank, world, local_rank):
     """Learned proposal workload: n=56 random degree<=3 graph (seeded order, max rank <= 28),
     MADE 2x512 trained on 2^16 exact samples + their exact conditionals; 4096 samples from
@@ -901,8 +977,8 @@ def main():
     ap.add_argument("--only", choices=["both", "c64", "c128"], default="both",
                     help="run only one precision (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
-    ap.add_argument("--workload", choices=["amplitudes", "fourier", "chain", "learned", "batched", "rgs70"], default="amplitudes")
-    ap.add_argument("--samples", type=int, default=4096, help="accepted samples of the learned workload")
+    ap.add_argument("--workload", choices=["amplitudes", "fourier", "chain", "learned", "batched", "rgs70", "full"], default="amplitudes")
+    ap.add_argument("--samples", type=int, default=4096, help="learned: accepted samples; full: exact samples")
     ap.add_argument("--epochs", type=int, default=8, help="training epochs of the learned workload")
     ap.add_argument("--m", type=int, default=30, help="conditional qubits of the fourier workload")
     ap.add_argument("--tile64", type=int, default=None, help="complex64 batch tile (default: 256 c64f32, 128 c64)")
@@ -929,6 +1005,8 @@ def main():
         run_batched(args, rank, world, local_rank)
     elif args.workload == "rgs70":
         run_rgs70(args, rank, world, local_rank)
+    elif args.workload == "full":
+        run_full(args, rank, world, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
 
