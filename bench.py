@@ -199,9 +199,10 @@ def run_ours(args, rank, world, local_rank):
     rng = np.random.default_rng(BITS_SEED + rank)
     bits = pkg.instances.uniform_bits(BATCH, N_QUBITS, rng)
     packed = pkg.pack_bits(bits, N_QUBITS)
-    bulk_tile = args.tile64 or (256 if args.bulk == "c64f32" else 128)
-    tile64 = min(bulk_tile, 1 << max(0, (BATCH - 1).bit_length()))
-    tile128 = min(args.tile128, 1 << max(0, (BATCH - 1).bit_length()))
+    # Batch tiles: given, or chosen by the package's autotuner on this GPU (first sweep).
+    cap = 1 << max(0, (BATCH - 1).bit_length())
+    tile64 = min(args.tile64, cap) if args.tile64 else "tune"
+    tile128 = min(args.tile128, cap) if args.tile128 else "tune"
     use64, use128 = args.only in ("both", "c64"), args.only in ("both", "c128")
     eng64 = pkg.ScanEngine(plan, inst.u, device=device, precision=args.bulk, batch_tile=tile64) if use64 else None
     eng128 = pkg.ScanEngine(plan, inst.u, device=device, precision="c128", batch_tile=tile128) if use128 else None
@@ -220,6 +221,10 @@ def run_ours(args, rank, world, local_rank):
     # 42 launches per tile replay without host launch overhead.
     queue_step(stream)
     torch.cuda.synchronize(device)
+    tile64 = eng64.batch_tile if use64 else None
+    tile128 = eng128.batch_tile if use128 else None
+    tuning = {k: {str(t): r for t, r in e.tuning[1].items()} for k, e in ((args.bulk, eng64), ("c128", eng128))
+              if e is not None and e.tuning is not None}
     graphs = {"step": pkg.capture_graph(device, queue_step)}
     if use64:
         graphs["bulk"] = pkg.capture_graph(device, lambda s: eng64.run_bits(d_bits, v64, l64, stream=s))
@@ -370,6 +375,7 @@ def run_ours(args, rank, world, local_rank):
                                    "65536 uniform 40-bit strings, complex64 + FP64 recheck of every result",
                        "instance": inst.name, "rmax": inst.rmax, "sum_states": inst.sum_states,
                        "batch_per_gpu": BATCH, "batch_tile": {args.bulk: tile64, "c128": tile128},
+                       "autotune_items_per_s": tuning,
                        "precisions": args.only,
                        "bulk": ("complex64 tables, float32 arithmetic" if args.bulk == "c64f32"
                                 else "complex64 tables, float64 arithmetic (the reference recipe)"),
@@ -981,11 +987,11 @@ def main():
     ap.add_argument("--samples", type=int, default=4096, help="learned: accepted samples; full: exact samples")
     ap.add_argument("--epochs", type=int, default=8, help="training epochs of the learned workload")
     ap.add_argument("--m", type=int, default=30, help="conditional qubits of the fourier workload")
-    ap.add_argument("--tile64", type=int, default=None, help="complex64 batch tile (default: 256 c64f32, 128 c64)")
+    ap.add_argument("--tile64", type=int, default=None, help="complex64 batch tile (default: autotuned)")
     ap.add_argument("--bulk", choices=["c64f32", "c64"], default="c64f32",
                     help="complex64 bulk arithmetic: float32 (default) or float64")
     ap.add_argument("--no-alt", action="store_true", help="skip timing the other complex64 recipe")
-    ap.add_argument("--tile128", type=int, default=64)
+    ap.add_argument("--tile128", type=int, default=None, help="complex128 batch tile (default: autotuned)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus if args.gpus == 1 else 1))

@@ -8,7 +8,7 @@ sm_100a CUDA kernels in ``librgs_b200.so`` through the C ABI of
 from . import _lib
 from .plan import ScanPlan, Step, make_plan, future_masks, rank_profile, byte_tables, kernel_combos, \
     edges_from_graph, search_order
-from .scan_oracle import ScanEngine, ScanOracle, pack_bits, amplitudes_from, PRECISIONS, capture_graph
+from .scan_oracle import ScanEngine, ScanOracle, pack_bits, amplitudes_from, PRECISIONS, capture_graph, autotune_tile
 from . import instances
 from .samplers import ConditionalSampler, DrawRecorder, produce, fwht, product, block_mass
 from .chain import ChainSampler, unpack_bits
@@ -20,7 +20,7 @@ from .proposal import MadeProposal, rejection_sample, capped_rejection, calibrat
 
 __all__ = [
     "ScanPlan", "Step", "make_plan", "future_masks", "rank_profile", "byte_tables", "kernel_combos",
-    "edges_from_graph", "search_order", "ScanEngine", "ScanOracle", "pack_bits", "amplitudes_from", "PRECISIONS", "capture_graph",
+    "edges_from_graph", "search_order", "ScanEngine", "ScanOracle", "pack_bits", "amplitudes_from", "PRECISIONS", "capture_graph", "autotune_tile",
     "ConditionalSampler", "DrawRecorder", "produce", "fwht", "product", "block_mass", "ChainSampler", "unpack_bits", "ResidentBatch",
     "MadeProposal", "rejection_sample", "capped_rejection", "calibrate_envelope",
 ]

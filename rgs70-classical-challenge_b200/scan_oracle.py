@@ -19,7 +19,7 @@ import torch
 from . import _lib
 from .plan import ScanPlan, edges_from_graph
 
-__all__ = ["ScanEngine", "ScanOracle", "pack_bits", "PRECISIONS", "max_batch_tile", "capture_graph"]
+__all__ = ["ScanEngine", "ScanOracle", "pack_bits", "PRECISIONS", "max_batch_tile", "capture_graph", "autotune_tile"]
 
 PRECISIONS = {"c64": _lib.PREC_C64, "c64f32": _lib.PREC_C64_F32, "c128": _lib.PREC_C128}
 LN2 = math.log(2.0)
@@ -75,8 +75,52 @@ def _auto_tile(batch, rmax, esize, budget, cap):
     return bt
 
 
+_TUNED = {}
+
+
+def autotune_tile(engine, d_bits, candidates=None, sample=None, reps=2):
+    """Batch tile of ``engine`` chosen by measurement: each candidate (powers of two up to
+    the precision's maximum that fit the memory budget) sweeps the same sample of items
+    ``reps`` times after one warm-up sweep; the tile with the highest items per second
+    wins.  Results are cached per (plan rank profile, precision, device).  Returns
+    (tile, {tile: items_per_second})."""
+    plan = engine.plan
+    key = (plan.n, tuple(plan.ranks), engine.precision, str(engine.device),
+           torch.cuda.get_device_name(engine.device))
+    if key in _TUNED:
+        return _TUNED[key]
+    cap = max_batch_tile(engine.precision)
+    if candidates is None:
+        candidates = [t for t in (8, 16, 32, 64, 128, 256, 512) if t <= cap]
+    fits = [t for t in candidates if 2 * t * engine.esize * (1 << plan.rmax) <= engine.memory_budget]
+    if not fits:
+        fits = [1]
+    count = int(d_bits.shape[0])
+    sample = min(count, sample if sample is not None else 4 * max(fits))
+    bits = d_bits[:sample]
+    val, ls = engine.out_tensors(sample)
+    s = torch.cuda.current_stream(engine.device)
+    rates = {}
+    for t in fits:
+        engine.run_bits(bits, val, ls, stream=s, tile=t)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(reps):
+            engine.run_bits(bits, val, ls, stream=s, tile=t)
+        e1.record(s)
+        torch.cuda.synchronize(engine.device)
+        rates[t] = sample * reps / (e0.elapsed_time(e1) / 1e3)
+    best = max(rates, key=rates.get)
+    engine._ws = None  # keep only the chosen tile's workspace
+    engine.workspace(best)
+    _TUNED[key] = (best, rates)
+    return best, rates
+
+
 class ScanEngine:
-    """Executes one compiled plan on one GPU with a caller-visible torch workspace."""
+    """Executes one compiled plan on one GPU with a caller-visible torch workspace.
+    ``batch_tile="tune"`` picks the tile by measurement (``autotune_tile``) at the first
+    call with bitstrings."""
 
     def __init__(self, plan, u, device=0, precision="c64", batch_tile=None, memory_budget=None):
         if precision not in PRECISIONS:
@@ -100,11 +144,14 @@ class ScanEngine:
             free, _total = torch.cuda.mem_get_info(self.device)
         self.memory_budget = int(memory_budget if memory_budget is not None else min(0.45 * free, 96 * 2 ** 30))
         self.batch_tile = batch_tile
+        self.tuning = None
         self._ws = None
         self._ws_tile = None
 
     # -------------------------------------------------------------- workspace
     def tile_for(self, batch):
+        if self.batch_tile == "tune":
+            raise ValueError("the tile is chosen at the first run_bits call (batch_tile='tune')")
         if self.batch_tile is not None:
             return int(self.batch_tile)
         return _auto_tile(batch, self.plan.rmax, self.esize, self.memory_budget, max_batch_tile(self.precision))
@@ -133,6 +180,8 @@ class ScanEngine:
     def run_bits(self, d_bits, out_value, out_logscale, stream=None, tile=None):
         """Queue the sweep for device bits uint64 [B, 2] into device outputs (no sync)."""
         batch = int(d_bits.shape[0])
+        if tile is None and self.batch_tile == "tune":
+            self.batch_tile, self.tuning = autotune_tile(self, d_bits)
         tile = tile or self.tile_for(batch)
         ws = self.workspace(tile)
         s = stream if stream is not None else torch.cuda.current_stream(self.device)

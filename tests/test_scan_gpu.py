@@ -180,3 +180,18 @@ def test_rgs70_reference_records(pkg, fixtures, rgs70_records, fp64):
     ref = np.array([r["probability_c128"] for r in rows])
     rel = np.abs(p - ref) / ref
     assert rel.max() < (1e-12 if fp64 else 1e-4), rel
+
+
+def test_autotuned_tile(pkg):
+    """batch_tile='tune' measures the candidate tiles on this GPU and keeps the fastest;
+    the result does not depend on the tile (bitwise)."""
+    inst = pkg.instances.make_instance("reg3", 22, 9, pkg.rank_profile)
+    plan = pkg.ScanPlan(22, pkg.edges_from_graph(inst.g), inst.order)
+    bits = pkg.instances.uniform_bits(300, 22, np.random.default_rng(3))
+    for prec in ("c64f32", "c128"):
+        tuned = pkg.ScanEngine(plan, inst.u, precision=prec, batch_tile="tune")
+        val, ls = tuned.sweep_bits(bits)
+        best, rates = tuned.tuning
+        assert tuned.batch_tile == best and best in rates and rates[best] == max(rates.values())
+        ref = pkg.ScanEngine(plan, inst.u, precision=prec, batch_tile=8).sweep_bits(bits)
+        assert np.array_equal(val, ref[0]) and np.array_equal(ls, ref[1])
