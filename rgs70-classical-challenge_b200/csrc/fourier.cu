@@ -45,7 +45,8 @@ FourierPlan::~FourierPlan() {
   int prev = -1;
   cudaGetDevice(&prev);
   cudaSetDevice(device);
-  for (void* p : {d_lut_z, d_lut_a, d_lut_cols, d_uA, d_uB, d_rot, d_dg, d_dh, d_rg, d_rh})
+  for (void* p : {d_lut_z, d_lut_a, d_lut_cols, d_uA, d_uB, d_rot, d_dg, d_dh, d_rg, d_rh, d_tt_init, d_tt_phase,
+                  d_qsym_z, d_qsym_a})
     if (p) cudaFree(p);
   if (prev >= 0) cudaSetDevice(prev);
 }
@@ -55,6 +56,11 @@ namespace {
 // ------------------------------------------------------------------------------------- device
 enum InitKind : int { INIT_LOAD = 0, INIT_COV_GENERIC = 1, INIT_COV_SPECIAL = 2, INIT_PRODUCT = 3 };
 
+// Per-pass tables of a quadratic phase q (and, for the init, the covariant map b = N z)
+// over the tile-local bits f of a pass configuration: with the tile's varying bits zero
+// in `base`, b(base ^ f) = b(base) ^ mlo[f & 63] ^ mhi[f >> 6] and
+// q(base ^ f) = q(base) ^ qtab[f] ^ parity(L & f), L_a = parity(qsym[global(a)] & base)
+// (q is a polynomial of degree 2, so q(x ^ y) = q(x) ^ q(y) ^ x^T (Q + Q^T) y).
 struct PassParams {
   float2* v;
   int m, c, K, q;                 // tile = c low bits + K target bits at q
@@ -74,6 +80,10 @@ struct PassParams {
   const float2* rg;               // [m] per-bit ratios d_j(1) / d_j(0) of the dg diagonal
   const float2* rh;               // [m] per-bit ratios of the dh diagonal
   const float2* wspecf;           // [(m+1)^2] popcount weights as complex64
+  const TileTables* tt_init;      // init tables of this pass configuration (lut_z), or null
+  const unsigned long long* qsym_z;  // [m] rows of Q + Q^T of the init phase
+  const TileTables* tt_phase;     // q_A tables of this pass configuration, or null
+  const unsigned long long* qsym_a;  // [m] rows of Q_A + Q_A^T
   double* masses;                 // per tile or null
   int store;
 };
@@ -177,6 +187,43 @@ __device__ __forceinline__ void window_tables(float2 (*wt)[16], const PassParams
 
 __device__ __forceinline__ float2 window_factor(const float2 (*wt)[16], int f) {
   return cmulf(cmulf(wt[0][f & 15], wt[1][(f >> 4) & 15]), wt[2][(f >> 8) & 15]);
+}
+
+// Loads a pass's tables into shared memory and evaluates the tile constants: b(base)
+// (when `map`), q(base) and the 12-bit linear mask L of the cross term.
+__device__ __forceinline__ void tile_tables_setup(const PassParams& P, const TileTables* tt, const u64* lut,
+                                                  const u64* qsym, u64 base, int TB, bool map, TileTables& st,
+                                                  u64& b0, int& q0, unsigned& lmask) {
+  const int t = threadIdx.x;
+  for (int i = t; i < 128; i += blockDim.x) {
+    st.qtab[i] = __ldg(&tt->qtab[i]);
+    if (map && i < 64) {
+      st.mlo[i] = __ldg(&tt->mlo[i]);
+      st.mhi[i] = __ldg(&tt->mhi[i]);
+    }
+  }
+  if (t < 32) {
+    // Blocks of small tiles have fewer than 32 threads: vote over the lanes that exist.
+    const unsigned lanes = blockDim.x >= 32 ? 0xffffffffu : ((1u << blockDim.x) - 1u);
+    unsigned bitv = 0;
+    if (t < TB) bitv = __popcll(__ldg(qsym + local_to_global_bit(P, t)) & base) & 1;
+    const unsigned lm = __ballot_sync(lanes, bitv);
+    if (t == 0) {
+      u64 b = 0, pm = 0;
+      for (int cc = 0; cc < P.chunks; ++cc) {
+        const u64* e = lut + ((((u64)cc << 8) + ((base >> (8 * cc)) & 255ull)) << 1);
+        if (map) b ^= __ldg(e);
+        pm ^= __ldg(e + 1);
+      }
+      b0 = b;
+      q0 = __popcll(pm & (base | (1ull << 63))) & 1;
+      lmask = lm;
+    }
+  }
+}
+
+__device__ __forceinline__ int tile_q(const TileTables& st, int q0, unsigned lmask, int f) {
+  return q0 ^ (int)((st.qtab[f >> 5] >> (f & 31)) & 1u) ^ (__popc(lmask & (unsigned)f) & 1);
 }
 
 // Initial value at index z (fourier_covariant_sampler.py:78-86, init_specialization.py:196-214,
@@ -285,6 +332,10 @@ __device__ void tile_rounds(float2* sm, const PassParams& P, int TB, unsigned ma
 __global__ void __launch_bounds__(256, 3) fourier_pass_kernel(const __grid_constant__ PassParams P) {
   extern __shared__ float2 sm[];
   __shared__ float2 wt[3][16];  // window tables of a diagonal (see window_tables)
+  __shared__ TileTables s_tt;   // pass tables of the init map / a phase (see TileTables)
+  __shared__ u64 s_b0;
+  __shared__ int s_q0;
+  __shared__ unsigned s_lm;
   const int TB = P.c + P.K;
   const int nt = 1 << (TB - 4);
   const u64 tile = blockIdx.x;
@@ -292,7 +343,26 @@ __global__ void __launch_bounds__(256, 3) fourier_pass_kernel(const __grid_const
   const u64 varying = ((1ull << P.c) - 1ull) | (((1ull << P.K) - 1ull) << P.q);
   // Load (or compute) the tile: each thread owns 8 element pairs (16-byte accesses,
   // pairs are adjacent in memory because tile bit 0 is a contiguous bit).
-  if (P.init) {
+  if (P.init == INIT_COV_SPECIAL && P.tt_init) {
+    // Covariant init from the pass tables: per element two shared-memory map lookups,
+    // two popcounts, one phase bit and the popcount weight.
+    tile_tables_setup(P, P.tt_init, P.lut_z, P.qsym_z, base, TB, true, s_tt, s_b0, s_q0, s_lm);
+    __syncthreads();
+    const u64 b0 = s_b0;
+    const int q0 = s_q0;
+    const unsigned lm = s_lm;
+#pragma unroll 2
+    for (int k = 0; k < 8; ++k) {
+      const int f0 = 2 * (threadIdx.x + k * nt);
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int f = f0 + e;
+        const u64 b = b0 ^ s_tt.mlo[f & 63] ^ s_tt.mhi[(f >> 6) & 63];
+        const float2 w = __ldg(P.wspecf + __popcll(b) * (P.m + 1) + __popcll(b & P.outmask));
+        sm[pad(f)] = tile_q(s_tt, q0, lm, f) ? make_float2(-w.x, -w.y) : w;
+      }
+    }
+  } else if (P.init) {
     TileLut t;
     tile_lut(P.lut_z, P.chunks, base, varying, t);
 #pragma unroll 2
@@ -320,7 +390,26 @@ __global__ void __launch_bounds__(256, 3) fourier_pass_kernel(const __grid_const
     }
   }
   if (P.wht_mask) tile_rounds(sm, P, TB, P.wht_mask, true);
-  if (P.phase) {
+  if (P.phase && P.tt_phase) {
+    // q_A phase from the pass tables, times the diagonal dg when given.
+    __syncthreads();  // readers of s_tt (init) are done
+    tile_tables_setup(P, P.tt_phase, P.lut_a, P.qsym_a, base, TB, false, s_tt, s_b0, s_q0, s_lm);
+    if (P.dg) window_tables(wt, P, P.dg, P.rg, base, TB);
+    __syncthreads();
+    const int q0 = s_q0;
+    const unsigned lm = s_lm;
+    for (int k = 0; k < 8; ++k) {
+      const int f0 = 2 * (threadIdx.x + k * nt);
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int f = f0 + e;
+        float2 x = sm[pad(f)];
+        if (P.dg) x = cmulf(x, window_factor(wt, f));
+        if (tile_q(s_tt, q0, lm, f)) x = make_float2(-x.x, -x.y);
+        sm[pad(f)] = x;
+      }
+    }
+  } else if (P.phase) {
     // q_A phase (-1)^{q_A(z)}, times the diagonal dg when given.
     TileLut t;
     tile_lut(P.lut_a, P.chunks, base, varying, t);
@@ -729,6 +818,45 @@ bool euler_factors(const double* u, std::complex<double> g[2], std::complex<doub
   return err < 1e-9;
 }
 
+// Host evaluation of the chunk tables (as the device does): the map part b(z) and the
+// quadratic phase q(z).
+u64 host_lut_map(const std::vector<u64h>& lut, int chunks, u64 z) {
+  u64 b = 0;
+  for (int cc = 0; cc < chunks; ++cc) b ^= lut[(((size_t)cc << 8) + ((z >> (8 * cc)) & 255ull)) * 2];
+  return b;
+}
+int host_lut_q(const std::vector<u64h>& lut, int chunks, u64 z) {
+  u64 pm = 0;
+  for (int cc = 0; cc < chunks; ++cc) pm ^= lut[(((size_t)cc << 8) + ((z >> (8 * cc)) & 255ull)) * 2 + 1];
+  return __builtin_popcountll(pm & (z | (1ull << 63))) & 1;
+}
+
+// Pass tables (TileTables) of a tile whose local bit a sits at global bit
+// a < c ? a : q + (a - c), and the rows of Q + Q^T of the phase (see the kernel).
+void pass_tables(const std::vector<u64h>& lut, int chunks, int m, int c, int K, int q, bool map, TileTables& tt,
+                 std::vector<u64h>& qsym) {
+  const int TB = c + K;
+  auto global = [&](int f) {
+    u64 z = 0;
+    for (int a = 0; a < TB; ++a)
+      if ((f >> a) & 1) z |= 1ull << (a < c ? a : q + (a - c));
+    return z;
+  };
+  for (int i = 0; i < 64; ++i) {
+    tt.mlo[i] = (map && i < (1 << TB)) ? host_lut_map(lut, chunks, global(i)) : 0ull;
+    tt.mhi[i] = (map && (i << 6) < (1 << TB)) ? host_lut_map(lut, chunks, global(i << 6)) : 0ull;
+  }
+  for (int w = 0; w < 128; ++w) tt.qtab[w] = 0u;
+  for (int f = 0; f < (1 << TB); ++f)
+    if (host_lut_q(lut, chunks, global(f))) tt.qtab[f >> 5] |= 1u << (f & 31);
+  qsym.assign(m, 0);
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < m; ++j)
+      if (i != j && (host_lut_q(lut, chunks, (1ull << i) ^ (1ull << j)) ^ host_lut_q(lut, chunks, 1ull << i) ^
+                     host_lut_q(lut, chunks, 1ull << j)))
+        qsym[i] |= 1ull << j;
+}
+
 // Chunk tables of a diagonal over m bits: T[c][code] = prod over bits t of chunk c of
 // f_j[bit t of code], j = 8c + t.
 void diag_tables(int m, int chunks, const std::vector<std::complex<double>>& f, std::vector<float>& out) {
@@ -836,6 +964,19 @@ std::string fourier_build(int n, const uint8_t* graph, const double* unitaries, 
       p.rh[2 * j + 1] = (float)b.imag();
     }
   }
+  // Pass tables of the init (pass 0, contiguous) and of the q_A phase (its pass).
+  {
+    const int c0 = std::min(m, kTileBits);
+    pass_tables(p.lut_z, p.chunks, m, c0, 0, c0, true, p.tt_init, p.qsym_z);
+    const auto groups = strided_groups(m);
+    if (groups.empty()) {
+      pass_tables(p.lut_a, p.chunks, m, c0, 0, c0, false, p.tt_phase, p.qsym_a);
+    } else {
+      const auto g = groups.back();
+      const int K = g.second - g.first;
+      pass_tables(p.lut_a, p.chunks, m, kTileBits - K, K, g.first, false, p.tt_phase, p.qsym_a);
+    }
+  }
   p.ngroups = (int)strided_groups(m).size();
   status = RGS_OK;
   return "";
@@ -873,6 +1014,10 @@ int fourier_upload(FourierPlan& p, int device) {
   if ((rc = up(&p.d_lut_cols, p.lut_cols.data(), p.lut_cols.size() * 8))) return rc;
   if ((rc = up(&p.d_uA, p.uA.data(), p.uA.size() * 8))) return rc;
   if ((rc = up(&p.d_uB, p.uB.data(), p.uB.size() * 8))) return rc;
+  if ((rc = up(&p.d_tt_init, &p.tt_init, sizeof(TileTables)))) return rc;
+  if ((rc = up(&p.d_tt_phase, &p.tt_phase, sizeof(TileTables)))) return rc;
+  if ((rc = up(&p.d_qsym_z, p.qsym_z.data(), p.qsym_z.size() * 8))) return rc;
+  if ((rc = up(&p.d_qsym_a, p.qsym_a.data(), p.qsym_a.size() * 8))) return rc;
   if (p.rot_ok) {
     if ((rc = up(&p.d_rot, p.rot.data(), p.rot.size() * 4))) return rc;
     if ((rc = up(&p.d_dg, p.dg.data(), p.dg.size() * 4))) return rc;
@@ -905,6 +1050,12 @@ int fourier_compute(FourierPlan& p, uint64_t outB, void* state, void* ws, size_t
   P.outmask = outB;
   P.rg = (const float2*)p.d_rg;
   P.rh = (const float2*)p.d_rh;
+  if (p.specialized) {
+    P.tt_init = (const TileTables*)p.d_tt_init;
+    P.qsym_z = (const u64*)p.d_qsym_z;
+  }
+  P.tt_phase = (const TileTables*)p.d_tt_phase;
+  P.qsym_a = (const u64*)p.d_qsym_a;
   // Products as real rotations between the two Euler diagonals: dg with the q_A phase,
   // dh after the last products.
   const float2* dg = p.rot_ok ? (const float2*)p.d_dg : nullptr;

@@ -14,6 +14,12 @@ constexpr int kTileBits = 12;   // elements per tile = 2^12 (32 KiB of complex64
 constexpr int kLowBits = 3;     // contiguous low bits kept in strided tiles (64-byte runs)
 constexpr int kChunkBits = 8;   // lookup-table chunk width over z (init_specialization.py:160)
 
+// Per-pass tables of the init map and of a quadratic phase (see fourier.cu).
+struct TileTables {
+  unsigned long long mlo[64], mhi[64];
+  unsigned qtab[128];
+};
+
 struct FourierPlan {
   int n = 0, m = 0;
   std::vector<int> A, B;
@@ -35,6 +41,8 @@ struct FourierPlan {
   std::vector<float> rot;        // [m][2] (c, s)
   std::vector<float> dg, dh;     // [chunks][256][2] complex64 chunk products of g / h
   std::vector<float> rg, rh;     // [m][2] per-bit ratios g(1)/g(0), h(1)/h(0)
+  TileTables tt_init{}, tt_phase{};         // pass tables of the init (pass 0) and of the q_A phase pass
+  std::vector<unsigned long long> qsym_z, qsym_a;  // [m] rows of Q + Q^T of the two phases
   // Pass schedule (see fourier.cu).
   int ngroups = 0;               // strided target groups above the low tile
   // Device copies.
@@ -49,6 +57,10 @@ struct FourierPlan {
   void* d_dh = nullptr;          // float2 [chunks][256]
   void* d_rg = nullptr;          // float2 [m]
   void* d_rh = nullptr;          // float2 [m]
+  void* d_tt_init = nullptr;
+  void* d_tt_phase = nullptr;
+  void* d_qsym_z = nullptr;
+  void* d_qsym_a = nullptr;
   ~FourierPlan();
 };
 

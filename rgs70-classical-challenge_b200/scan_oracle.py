@@ -181,7 +181,8 @@ class ScanEngine:
         """Queue the sweep for device bits uint64 [B, 2] into device outputs (no sync)."""
         batch = int(d_bits.shape[0])
         if tile is None and self.batch_tile == "tune":
-            self.batch_tile, self.tuning = autotune_tile(self, d_bits)
+            self.tuning = autotune_tile(self, d_bits)
+            self.batch_tile = self.tuning[0]
         tile = tile or self.tile_for(batch)
         ws = self.workspace(tile)
         s = stream if stream is not None else torch.cuda.current_stream(self.device)
