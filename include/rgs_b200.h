@@ -206,6 +206,13 @@ int rgs_fourier_workspace_bytes(const rgs_fourier* plan, size_t* bytes);
  * float[3] for device times of (init, walsh, product) -- then the call synchronises. */
 int rgs_fourier_compute(rgs_fourier* plan, uint64_t outB, void* state, void* workspace, size_t workspace_bytes,
                         void* stream, float* stage_ms);
+/* Autotuning of the pass kernels for this plan: times a compute with each launch
+ * variant (3 or 4 resident blocks per SM) and keeps the faster (replaces the reference's
+ * fixed fusion_bits / chunk_mib choice, W/born_production.py:34).  *variant = the chosen
+ * one, ms[2] = milliseconds per compute of each (may be NULL).  Overwrites `state`;
+ * synchronises. */
+int rgs_fourier_tune(rgs_fourier* plan, void* state, void* workspace, size_t workspace_bytes, void* stream,
+                     int32_t* variant, float* ms);
 /* The reference base pipeline (distributed_sampler.py:126-144): product init over b,
  * WHT, index map with q_A phase into `scratch`, products; result in `scratch`. */
 int rgs_fourier_compute_permute(rgs_fourier* plan, uint64_t outB, void* state, void* scratch, void* workspace,

@@ -104,6 +104,8 @@ SIGNATURES = {
                                         c_int32_p]),
     "rgs_fourier_tables": (ctypes.c_int, [c_void_p, c_uint64_p, c_uint64_p, c_uint64_p, c_uint64_p, c_int32_p]),
     "rgs_fourier_workspace_bytes": (ctypes.c_int, [c_void_p, c_size_t_p]),
+    "rgs_fourier_tune": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_size_t, c_void_p, c_int32_p,
+                                        ctypes.POINTER(ctypes.c_float)]),
     "rgs_fourier_compute": (ctypes.c_int, [c_void_p, ctypes.c_uint64, c_void_p, c_void_p, ctypes.c_size_t, c_void_p,
                                            ctypes.POINTER(ctypes.c_float)]),
     "rgs_fourier_compute_permute": (ctypes.c_int, [c_void_p, ctypes.c_uint64, c_void_p, c_void_p, c_void_p,

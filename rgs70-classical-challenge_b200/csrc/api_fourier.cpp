@@ -73,6 +73,14 @@ int rgs_fourier_workspace_bytes(const rgs_fourier* f, size_t* bytes) {
   return RGS_OK;
 }
 
+int rgs_fourier_tune(rgs_fourier* f, void* state, void* workspace, size_t workspace_bytes, void* stream,
+                     int32_t* variant, float* ms) {
+  if (!f) return fail(RGS_ERR_ARG, "plan is NULL");
+  int rc = fourier_tune(f->plan, state, workspace, workspace_bytes, (cudaStream_t)stream, ms);
+  if (!rc && variant) *variant = f->plan.variant;
+  return rc;
+}
+
 int rgs_fourier_compute(rgs_fourier* f, uint64_t outB, void* state, void* workspace, size_t workspace_bytes,
                         void* stream, float* stage_ms) {
   if (!f) return fail(RGS_ERR_ARG, "plan is NULL");

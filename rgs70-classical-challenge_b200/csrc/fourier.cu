@@ -84,6 +84,7 @@ struct PassParams {
   const unsigned long long* qsym_z;  // [m] rows of Q + Q^T of the init phase
   const TileTables* tt_phase;     // q_A tables of this pass configuration, or null
   const unsigned long long* qsym_a;  // [m] rows of Q_A + Q_A^T
+  int variant;                    // launch variant (see fourier_pass_kernel)
   double* masses;                 // per tile or null
   int store;
 };
@@ -329,7 +330,10 @@ __device__ void tile_rounds(float2* sm, const PassParams& P, int TB, unsigned ma
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(256, 3) fourier_pass_kernel(const __grid_constant__ PassParams P) {
+// MINB resident blocks per SM: 3 (80 registers, no spills) or 4 (64 registers, a few
+// spilled); the plan's tuned variant picks one (fourier_tune).
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) fourier_pass_kernel(const __grid_constant__ PassParams P) {
   extern __shared__ float2 sm[];
   __shared__ float2 wt[3][16];  // window tables of a diagonal (see window_tables)
   __shared__ TileTables s_tt;   // pass tables of the init map / a phase (see TileTables)
@@ -653,13 +657,14 @@ __global__ void __launch_bounds__(1024) fourier_draw_kernel(const double* __rest
 // ------------------------------------------------------------------------------------- host
 std::mutex g_fourier_mutex;
 
+template <int MINB>
 int set_smem_attr() {
   static bool done[64] = {false};
   int device = 0;
   RGS_CUDA_TRY(cudaGetDevice(&device));
   std::lock_guard<std::mutex> lock(g_fourier_mutex);
   if (device >= 0 && device < 64 && done[device]) return RGS_OK;
-  RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_pass_kernel<MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     ((1 << kTileBits) + (1 << (kTileBits - 4))) * (int)sizeof(float2)));
   if (device >= 0 && device < 64) done[device] = true;
   return RGS_OK;
@@ -669,9 +674,13 @@ int launch_pass(const PassParams& P, cudaStream_t s) {
   const int TB = P.c + P.K;
   if (TB < 4 || TB > kTileBits) return fail(RGS_ERR_UNSUPPORTED, "tile must span 4..13 bits");
   const u64 tiles = 1ull << (P.m - TB);
-  int rc = set_smem_attr();
+  const size_t smem = ((1 << TB) + (1 << (TB - 4))) * sizeof(float2);
+  int rc = P.variant ? set_smem_attr<4>() : set_smem_attr<3>();
   if (rc) return rc;
-  fourier_pass_kernel<<<(unsigned)tiles, 1 << (TB - 4), ((1 << TB) + (1 << (TB - 4))) * sizeof(float2), s>>>(P);
+  if (P.variant)
+    fourier_pass_kernel<4><<<(unsigned)tiles, 1 << (TB - 4), smem, s>>>(P);
+  else
+    fourier_pass_kernel<3><<<(unsigned)tiles, 1 << (TB - 4), smem, s>>>(P);
   RGS_CUDA_TRY(cudaGetLastError());
   return RGS_OK;
 }
@@ -1056,6 +1065,7 @@ int fourier_compute(FourierPlan& p, uint64_t outB, void* state, void* ws, size_t
   }
   P.tt_phase = (const TileTables*)p.d_tt_phase;
   P.qsym_a = (const u64*)p.d_qsym_a;
+  P.variant = p.variant;
   // Products as real rotations between the two Euler diagonals: dg with the q_A phase,
   // dh after the last products.
   const float2* dg = p.rot_ok ? (const float2*)p.d_dg : nullptr;
@@ -1118,6 +1128,36 @@ int fourier_compute(FourierPlan& p, uint64_t outB, void* state, void* ws, size_t
     cudaEventElapsedTime(&stages->product_ms, ev[2], ev[3]);
     for (auto& e : ev) cudaEventDestroy(e);
   }
+  return RGS_OK;
+}
+
+int fourier_tune(FourierPlan& p, void* state, void* ws, size_t ws_bytes, cudaStream_t s, float* ms) {
+  cudaEvent_t e0, e1;
+  RGS_CUDA_TRY(cudaEventCreate(&e0));
+  RGS_CUDA_TRY(cudaEventCreate(&e1));
+  float best = 0.f;
+  int chosen = 0;
+  for (int v = 0; v < 2; ++v) {
+    p.variant = v;
+    int rc = fourier_compute(p, 0, state, ws, ws_bytes, s, nullptr);
+    if (rc) return rc;
+    RGS_CUDA_TRY(cudaEventRecord(e0, s));
+    for (int r = 0; r < 2; ++r)
+      if ((rc = fourier_compute(p, 0, state, ws, ws_bytes, s, nullptr))) return rc;
+    RGS_CUDA_TRY(cudaEventRecord(e1, s));
+    RGS_CUDA_TRY(cudaEventSynchronize(e1));
+    float t = 0.f;
+    RGS_CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+    t *= 0.5f;
+    if (ms) ms[v] = t;
+    if (v == 0 || t < best) {
+      best = t;
+      chosen = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  p.variant = chosen;
   return RGS_OK;
 }
 

@@ -25,6 +25,7 @@ struct FourierPlan {
   std::vector<int> A, B;
   bool specialized = false;      // all U_B identical: popcount weight table (init_specialization.py)
   bool deferred = true;          // terminal unitary on bit m-1 applied at draw time
+  int variant = 0;               // pass-kernel launch variant (fourier_tune)
   int chunks = 0;
   std::vector<u64h> lut_z;       // [chunks][256][2] covariant map + transformed q_B
   std::vector<u64h> lut_a;       // [chunks][256][2] q_A phase (entry[0] = 0)
@@ -82,6 +83,10 @@ struct FourierStages {
 // Full conditional state for outcome mask outB (bit j = outcome of B_j), in place in
 // `state` (complex64[2^m]); tile masses into the workspace.  If `stages` is given the
 // call synchronises and reports device time per stage.
+// Times one compute with each pass-kernel variant (after a warm-up) and keeps the faster
+// for this plan; ms[v] = milliseconds per compute (may be null).  Synchronises.
+int fourier_tune(FourierPlan& p, void* state, void* ws, size_t ws_bytes, cudaStream_t s, float* ms);
+
 int fourier_compute(FourierPlan& p, uint64_t outB, void* state, void* ws, size_t ws_bytes, cudaStream_t s,
                     FourierStages* stages);
 // Reference pipeline (W/distributed_sampler.py:126-144, single device): product init over

@@ -149,6 +149,18 @@ class ConditionalSampler:
             self.sync()
             return {"permute_pipeline": time.perf_counter() - start}
 
+    def tune(self):
+        """Times one compute per pass-kernel launch variant on this GPU and keeps the
+        faster for this sampler (overwrites the state).  Returns (variant, ms per variant)."""
+        v = ctypes.c_int32()
+        ms = (ctypes.c_float * 2)()
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.lib().rgs_fourier_tune(self._h, ctypes.c_void_p(self.state.data_ptr()),
+                                                   ctypes.c_void_p(self.workspace.data_ptr()), self.workspace.numel(),
+                                                   _stream(self.device), ctypes.byref(v), ms))
+        self.variant = int(v.value)
+        return self.variant, [float(ms[0]), float(ms[1])]
+
     def masses(self):
         """(tile masses float64, norm, tilebits, nmass); raises if |norm - 1| > 1e-3."""
         out = np.zeros(self.nmass, dtype=np.float64)
