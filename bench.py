@@ -196,7 +196,8 @@ def run_ours(args, rank, world, local_rank):
         dist.init_process_group("nccl", device_id=device)
 
     plan = pkg.ScanPlan(N_QUBITS, pkg.edges_from_graph(inst.g), inst.order)
-    rng = np.random.default_rng(BITS_SEED + rank)
+    # Replicas: every rank evaluates its own strings from its own seed stream.
+    rng = np.random.default_rng(pkg.replicas.rank_seeds(BITS_SEED, world)[rank] if world > 1 else BITS_SEED)
     bits = pkg.instances.uniform_bits(BATCH, N_QUBITS, rng)
     packed = pkg.pack_bits(bits, N_QUBITS)
     # Batch tiles: given, or chosen by the package's autotuner on this GPU (first sweep).
@@ -239,11 +240,7 @@ def run_ours(args, rank, world, local_rank):
             dist.barrier()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return pkg.replicas.max_over_ranks(x, device=device)
 
     def timed(fn, k):
         barrier()

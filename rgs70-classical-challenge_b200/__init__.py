@@ -15,6 +15,7 @@ from .chain import ChainSampler, unpack_bits
 from .batch import ResidentBatch
 from . import batch
 from . import frontend
+from . import replicas
 from . import proposal
 from .proposal import MadeProposal, rejection_sample, capped_rejection, calibrate_envelope
 
