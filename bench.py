@@ -490,7 +490,7 @@ def run_chain(args, rank, world, local_rank, emit=True):
     torch.cuda.set_device(device)
     if world > 1 and not dist.is_initialized():
         dist.init_process_group("nccl", device_id=device)
-    chain_tile = args.tile64 or 128
+    chain_tile = min(args.tile64 or 128, 128)
     cs = pkg.ChainSampler(inst.g, inst.u, inst.order, device=device, precision="c64", batch_tile=chain_tile)
     stream = torch.cuda.current_stream(device)
     outs = cs._outs(BATCH)
