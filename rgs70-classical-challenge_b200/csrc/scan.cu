@@ -182,9 +182,10 @@ __global__ void scan_finalize_kernel(const S* __restrict__ E, const u64* __restr
 }
 
 // ------------------------------------------------------------------------------------------------
-// Largest batch tile per precision: a lane owns at most 2 chunks (4 for float32 math).
+// Largest batch tile per precision: a lane owns at most 4 chunks (complex128: gathered
+// two at a time) or, with float32 arithmetic, 4 chunks of two items.
 int scan_max_tile(int precision) {
-  if (precision == RGS_PREC_C128) return 64;
+  if (precision == RGS_PREC_C128) return 128;
   if (precision == RGS_PREC_C64_F32) return 256;
   return 128;
 }
@@ -257,7 +258,8 @@ StepGeometry step_geometry(int precision, int Bt, const DevStep& st, int device)
   const int lL = lC < 5 ? lC : 5;
   g.CPL = 1 << (lC - lL);
   const int loads = precision == RGS_PREC_C64 ? 4 : 8;  // LoadsInFlight of the kernel
-  const int U = (st.ncombos * g.CPL >= loads) ? 1 : loads / (st.ncombos * g.CPL);
+  const int group = std::min(g.CPL, (precision == RGS_PREC_C64_F32) ? 4 : 2);  // ChunkGroup of the kernel
+  const int U = (st.ncombos * group >= loads) ? 1 : loads / (st.ncombos * group);
   const unsigned long long items = st.mode == MODE_PAIR ? (1ull << (st.r_out - 1)) : (1ull << st.r_out);
   const unsigned long long per_warp = (unsigned long long)U << (5 - lL);
   const unsigned long long warps = (items + per_warp - 1) / per_warp;
@@ -274,7 +276,8 @@ cudaError_t launch_step(int precision, int Bt, int device, cudaStream_t s, const
   const dim3 grid((unsigned)g.blocks);
   if (precision == RGS_PREC_C128) {
     if (g.CPL == 1) return launch_modes<double, double, 1, 1>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
-    return launch_modes<double, double, 1, 2>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+    if (g.CPL == 2) return launch_modes<double, double, 1, 2>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+    return launch_modes<double, double, 1, 4>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
   }
   if (precision == RGS_PREC_C64) {
     if (g.VE == 1) return launch_modes<float, double, 1, 1>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);

@@ -38,6 +38,14 @@ template <typename S, typename M>
 struct LoadsInFlight {
   static constexpr int value = sizeof(M) > sizeof(S) ? 4 : 8;
 };
+// Chunks of a row a lane gathers at once: all CPL of them up to two (complex128 or
+// float64 arithmetic) or four (float32 arithmetic) -- longer rows are walked in groups,
+// with the row's index work still done once per lane.
+template <typename S, typename M, int CPL>
+struct ChunkGroup {
+  static constexpr int cap = (sizeof(S) == 8 || sizeof(M) == 8) ? 2 : 4;
+  static constexpr int value = CPL < cap ? CPL : cap;
+};
 
 // x with its sign flipped iff neg (exact).
 __device__ __forceinline__ float flip_sign(float x, int neg) {
@@ -54,7 +62,8 @@ __global__ void __launch_bounds__(256, 2) scan_row_kernel(const S* __restrict__ 
                                                        const unsigned char* __restrict__ F,
                                                        const u64* __restrict__ maxprev, u64* __restrict__ maxcur,
                                                        int lbt, int unit_input) {
-  constexpr int U = RowsPerIter<NC, CPL, LoadsInFlight<S, M>::value>::value;
+  constexpr int CPLG = ChunkGroup<S, M, CPL>::value;
+  constexpr int U = RowsPerIter<NC, CPLG, LoadsInFlight<S, M>::value>::value;
   constexpr int NI = CPL * VE;             // items owned by a lane
   __shared__ u64 smax[256];
   const int Bt = 1 << lbt;
@@ -116,7 +125,7 @@ __global__ void __launch_bounds__(256, 2) scan_row_kernel(const S* __restrict__ 
     u64 cc[U][NC];
     int pc[U][NC];
     bool ok[U];
-    Chunk<S, VE> e[U][NC][CPL];
+    Chunk<S, VE> e[U][NC][CPLG];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const u64 it = base + ((u64)u << lR) + sub;
@@ -141,68 +150,72 @@ __global__ void __launch_bounds__(256, 2) scan_row_kernel(const S* __restrict__ 
         pc[u][k] = __popcll(cc[u][k] & st.beta) & 1;
       }
     }
-    // All gathers of this iteration before any arithmetic.
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
+    for (int g = 0; g < CPL; g += CPLG) {
+      // All gathers of this chunk group before any arithmetic.
 #pragma unroll
-      for (int k = 0; k < NC; ++k) {
+      for (int u = 0; u < U; ++u) {
 #pragma unroll
-        for (int j = 0; j < CPL; ++j) {
-          if (unit_input || !ok[u])
-            e[u][k][j].unit();
-          else
-            e[u][k][j].load(Ein, (cc[u][k] << lC) + (u64)(l + (j << lL)));
+        for (int k = 0; k < NC; ++k) {
+#pragma unroll
+          for (int jj = 0; jj < CPLG; ++jj) {
+            if (unit_input || !ok[u])
+              e[u][k][jj].unit();
+            else
+              e[u][k][jj].load(Ein, (cc[u][k] << lC) + (u64)(l + ((g + jj) << lL)));
+          }
         }
       }
-    }
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (!ok[u]) continue;
+      for (int u = 0; u < U; ++u) {
+        if (!ok[u]) continue;
 #pragma unroll
-      for (int j = 0; j < CPL; ++j) {
-        Chunk<S, VE> outA, outB;
+        for (int jj = 0; jj < CPLG; ++jj) {
+          const int j = g + jj;
+          Chunk<S, VE> outA, outB;
 #pragma unroll
-        for (int v = 0; v < VE; ++v) {
-          const int i = j * VE + v;
-          Cx<M> oa{(M)0, (M)0}, ob{(M)0, (M)0};
+          for (int v = 0; v < VE; ++v) {
+            const int i = j * VE + v;
+            Cx<M> oa{(M)0, (M)0}, ob{(M)0, (M)0};
 #pragma unroll
-          for (int k = 0; k < NC; ++k) {
-            const int par = pc[u][k] ^ ov[i];
-            if (MODE == MODE_PAIR) {
-              const M pr = (M)e[u][k][j].re(v), pi = (M)e[u][k][j].im(v);
-              const M nr = flip_sign(pr, par), ni = flip_sign(pi, par);
-              if (k < NG0) {
-                cmad(oa, pr, pi, wA[i]);
-                cmad(ob, nr, ni, wB[i]);
+            for (int k = 0; k < NC; ++k) {
+              const int par = pc[u][k] ^ ov[i];
+              if (MODE == MODE_PAIR) {
+                const M pr = (M)e[u][k][jj].re(v), pi = (M)e[u][k][jj].im(v);
+                const M nr = flip_sign(pr, par), ni = flip_sign(pi, par);
+                if (k < NG0) {
+                  cmad(oa, pr, pi, wA[i]);
+                  cmad(ob, nr, ni, wB[i]);
+                } else {
+                  cmad(oa, nr, ni, wB[i]);
+                  cmad(ob, pr, pi, wA[i]);
+                }
+              } else if (MODE == MODE_MERGE) {
+                const M er = (M)e[u][k][jj].re(v), ei = (M)e[u][k][jj].im(v);
+                cmad(oa, er, ei, par ? wB[i] : wA[i]);
               } else {
-                cmad(oa, nr, ni, wB[i]);
-                cmad(ob, pr, pi, wA[i]);
+                const M er = (M)e[u][k][jj].re(v), ei = (M)e[u][k][jj].im(v);
+                Cx<M> w = wA[i];
+                if (yf[i] & par) {
+                  w.re = -w.re;
+                  w.im = -w.im;
+                }
+                cmad(oa, er, ei, w);
               }
-            } else if (MODE == MODE_MERGE) {
-              const M er = (M)e[u][k][j].re(v), ei = (M)e[u][k][j].im(v);
-              cmad(oa, er, ei, par ? wB[i] : wA[i]);
-            } else {
-              const M er = (M)e[u][k][j].re(v), ei = (M)e[u][k][j].im(v);
-              Cx<M> w = wA[i];
-              if (yf[i] & par) {
-                w.re = -w.re;
-                w.im = -w.im;
-              }
-              cmad(oa, er, ei, w);
+            }
+            const S ar = (S)oa.re, ai = (S)oa.im;
+            outA.set(v, ar, ai);
+            mx[i] = fmax(mx[i], norm2(ar, ai));
+            if (MODE == MODE_PAIR) {
+              const S br = (S)ob.re, bi = (S)ob.im;
+              outB.set(v, br, bi);
+              mx[i] = fmax(mx[i], norm2(br, bi));
             }
           }
-          const S ar = (S)oa.re, ai = (S)oa.im;
-          outA.set(v, ar, ai);
-          mx[i] = fmax(mx[i], norm2(ar, ai));
-          if (MODE == MODE_PAIR) {
-            const S br = (S)ob.re, bi = (S)ob.im;
-            outB.set(v, br, bi);
-            mx[i] = fmax(mx[i], norm2(br, bi));
-          }
+          const u64 col = (u64)(l + (j << lL));
+          outA.store(Eout, (ca[u] << lC) + col);
+          if (MODE == MODE_PAIR) outB.store(Eout, (cb[u] << lC) + col);
         }
-        const u64 col = (u64)(l + (j << lL));
-        outA.store(Eout, (ca[u] << lC) + col);
-        if (MODE == MODE_PAIR) outB.store(Eout, (cb[u] << lC) + col);
       }
     }
   }
