@@ -609,6 +609,7 @@ def run_batched(args, rank, world, local_rank):
         c, d = k * S, (k + 1) * S
         rb.add_device(plan, du, d_bits[a:b], value[a:b], logscale[a:b], S, 5000 + 7919 * k + rank,
                       sbits[c:d], svalue[c:d], slogscale[c:d], slogp[c:d])
+    variant, tune_ms = rb.tune()
     rb.capture()
     stream = torch.cuda.current_stream(device)
     for _ in range(args.warmup):
@@ -670,7 +671,9 @@ def run_batched(args, rank, world, local_rank):
                                    f"{min(i.rmax for i in insts)}-{max(i.rmax for i in insts)}): {K} amplitudes + "
                                    f"{S} samples each per step, one persistent launch replayed from a CUDA graph",
                        "instances": nI, "strings_per_instance": K, "samples_per_instance": S,
-                       "work_units": rb.units, "l2": "tables live in shared memory; HBM holds only inputs and outputs"},
+                       "work_units": rb.units, "l2": "tables live in shared memory; HBM holds only inputs and outputs",
+                       "tuned_variant": {"chosen": ["512 threads, 1 block/SM", "256 threads, 2 blocks/SM"][variant],
+                                         "ms_per_run": tune_ms}},
             "roofline": {"bound": "smem", "achieved": tb * args.steps / t / 1e9, "peak": smem_peak, "unit": "GB/s",
                          "frac": tb * args.steps / t / 1e9 / smem_peak, "traffic": None,
                          "note": "table bytes through shared memory vs the nominal shared-memory bandwidth"},

@@ -85,6 +85,7 @@ SIGNATURES = {
                                      c_int32_p]),
     "rgs_batch_info": (ctypes.c_int, [c_void_p, c_int32_p, ctypes.POINTER(ctypes.c_int64)]),
     "rgs_batch_run": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_void_p]),
+    "rgs_batch_tune": (ctypes.c_int, [c_void_p, c_void_p, c_int32_p, ctypes.POINTER(ctypes.c_float)]),
     "rgs_gemm_bf16": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_void_p, ctypes.c_int32,
                                      ctypes.c_int32, c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_float,
                                      c_void_p, ctypes.c_int32, c_void_p, c_void_p, c_void_p, c_void_p,

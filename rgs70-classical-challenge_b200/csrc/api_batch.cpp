@@ -11,6 +11,7 @@
 
 struct rgs_batch {
   int precision = RGS_PREC_C64;
+  int variant = 0;  // launch variant (rgs_batch_tune)
   std::vector<rgs::ResInstance> insts;
   rgs::ResDevice dev;
   bool dirty = true;
@@ -99,6 +100,7 @@ int rgs_batch_add(rgs_batch* batch, rgs_plan* plan, const double* unitaries, con
   in.nb = nb;
   in.rmax = p.rmax;
   in.has_fixed = fixed ? 1 : 0;
+  if (resident_items(p.rmax, batch->precision, batch->variant) < 1) batch->variant = 0;  // the tuned variant is too small
   if (index) *index = (int32_t)batch->insts.size();
   batch->insts.push_back(in);
   batch->units += (count + nb - 1) / nb + (nsamples + nb - 1) / nb;
@@ -113,12 +115,57 @@ int rgs_batch_info(const rgs_batch* batch, int32_t* instances, int64_t* units) {
   return RGS_OK;
 }
 
+int rgs_batch_tune(rgs_batch* batch, void* stream, int32_t* variant, float* ms) {
+  if (!batch) return fail(RGS_ERR_ARG, "null batch");
+  if (batch->insts.empty()) return RGS_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  int best = -1;
+  float best_ms = 0.f;
+  for (int v = 0; v < kResVariants; ++v) {
+    if (ms) ms[v] = -1.f;
+    bool fits = true;
+    for (auto& in : batch->insts)
+      if (resident_items(in.rmax, batch->precision, v) < 1) fits = false;
+    if (!fits) continue;
+    int rc = resident_prepare(batch->insts, batch->precision, v, batch->dev);
+    if (rc) return rc;
+    if ((rc = resident_launch(batch->dev, batch->precision, s, nullptr))) return rc;
+    cudaEvent_t e0, e1;
+    RGS_CUDA_TRY(cudaEventCreate(&e0));
+    RGS_CUDA_TRY(cudaEventCreate(&e1));
+    RGS_CUDA_TRY(cudaEventRecord(e0, s));
+    for (int r = 0; r < 2; ++r)
+      if ((rc = resident_launch(batch->dev, batch->precision, s, nullptr))) return rc;
+    RGS_CUDA_TRY(cudaEventRecord(e1, s));
+    RGS_CUDA_TRY(cudaEventSynchronize(e1));
+    float t = 0.f;
+    RGS_CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    t *= 0.5f;
+    if (ms) ms[v] = t;
+    if (best < 0 || t < best_ms) {
+      best = v;
+      best_ms = t;
+    }
+  }
+  if (best < 0) return fail(RGS_ERR_UNSUPPORTED, "no launch variant holds every instance");
+  batch->variant = best;
+  int rc = resident_prepare(batch->insts, batch->precision, best, batch->dev);
+  if (rc) return rc;
+  batch->units = batch->dev.nwork;
+  batch->dirty = false;
+  if (variant) *variant = best;
+  return RGS_OK;
+}
+
 int rgs_batch_run(rgs_batch* batch, int32_t check, void* stream) {
   if (!batch) return fail(RGS_ERR_ARG, "null batch");
   if (batch->insts.empty()) return RGS_OK;
   int rc;
   if (batch->dirty) {
-    if ((rc = resident_prepare(batch->insts, batch->precision, batch->dev))) return rc;
+    if ((rc = resident_prepare(batch->insts, batch->precision, batch->variant, batch->dev))) return rc;
+    batch->units = batch->dev.nwork;
     batch->dirty = false;
   }
   cudaStream_t s = (cudaStream_t)stream;

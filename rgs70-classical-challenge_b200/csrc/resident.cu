@@ -198,8 +198,8 @@ __device__ __forceinline__ void fold_max(const u64* redm, int tid, int lnb, int 
 // previous position's maximum, then the weights of an amplitude unit; thread 0: the next
 // step record), a barrier, [sample units: decision and weights, a barrier], the step
 // (rows of the chosen branch, per-thread maxima), a barrier.
-template <typename S, typename M>
-__global__ void __launch_bounds__(kResThreads, 1)
+template <typename S, typename M, int kResThreads, int kResidentSmem>
+__global__ void __launch_bounds__(kResThreads, 512 / kResThreads)
     resident_kernel(const ResInstance* __restrict__ insts, const ResWork* __restrict__ work, long long nwork,
                     int* __restrict__ counter) {
   typedef typename Pair2<S>::T V;
@@ -396,48 +396,58 @@ __global__ void __launch_bounds__(kResThreads, 1)
   }
 }
 
-template <typename S, typename M>
-int launch_kernel(const ResDevice& dev, cudaStream_t stream, int blocks) {
+template <typename S, typename M, int V>
+int launch_variant(const ResDevice& dev, cudaStream_t stream, int blocks) {
+  constexpr int T = kResThreadsOf[V], SM = kResSmemOf[V];
   static std::mutex mu;
   static bool attr_set[64] = {false};
   {
     std::lock_guard<std::mutex> lock(mu);
     if (dev.device >= 0 && dev.device < 64 && !attr_set[dev.device]) {
-      RGS_CUDA_TRY(cudaFuncSetAttribute(resident_kernel<S, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        kResidentSmem));
+      RGS_CUDA_TRY(cudaFuncSetAttribute(resident_kernel<S, M, T, SM>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM));
       attr_set[dev.device] = true;
     }
   }
-  resident_kernel<S, M><<<blocks, kResThreads, kResidentSmem, stream>>>(dev.insts, dev.work, dev.nwork,
-                                                                        dev.counter);
+  resident_kernel<S, M, T, SM><<<blocks, T, SM, stream>>>(dev.insts, dev.work, dev.nwork, dev.counter);
   RGS_CUDA_TRY(cudaGetLastError());
   return RGS_OK;
 }
 
-size_t table_entries(int precision) {
+template <typename S, typename M>
+int launch_kernel(const ResDevice& dev, cudaStream_t stream, int blocks) {
+  return dev.variant ? launch_variant<S, M, 1>(dev, stream, blocks) : launch_variant<S, M, 0>(dev, stream, blocks);
+}
+
+size_t table_entries(int precision, int variant) {
   const size_t esize = precision == RGS_PREC_C128 ? 16 : 8;
-  return (size_t)kResidentSmem / (2 * esize);
+  return (size_t)kResSmemOf[variant] / (2 * esize);
 }
 
 }  // namespace
 
-int resident_max_rank(int precision) {
-  const size_t cap = table_entries(precision);
+int resident_max_rank(int precision, int variant) {
+  const size_t cap = table_entries(precision, variant);
   int r = 0;
   while (((size_t)2 << r) <= cap) ++r;
   return r;
 }
 
-int resident_items(int rmax, int precision) {
-  if (rmax < 0 || rmax > resident_max_rank(precision)) return 0;
-  const size_t cap = table_entries(precision);
+int resident_items(int rmax, int precision, int variant) {
+  if (rmax < 0 || rmax > resident_max_rank(precision, variant)) return 0;
+  const size_t cap = table_entries(precision, variant);
   int nb = kMaxResItems;
   while (nb > 1 && ((size_t)nb << rmax) > cap) nb >>= 1;
   return nb;
 }
 
-int resident_prepare(const std::vector<ResInstance>& insts, int precision, ResDevice& dev) {
+int resident_prepare(const std::vector<ResInstance>& insts_in, int precision, int variant, ResDevice& dev) {
   if (dev.device < 0) return fail(RGS_ERR_ARG, "batch has no device");
+  if (variant < 0 || variant >= kResVariants) return fail(RGS_ERR_ARG, "unknown launch variant");
+  std::vector<ResInstance> insts(insts_in);
+  for (auto& in : insts) {
+    in.nb = resident_items(in.rmax, precision, variant);
+    if (in.nb < 1) return fail(RGS_ERR_UNSUPPORTED, "an instance's tables do not fit this launch variant");
+  }
   std::vector<ResWork> work;
   std::vector<double> cost;
   for (size_t i = 0; i < insts.size(); ++i) {
@@ -484,6 +494,7 @@ int resident_prepare(const std::vector<ResInstance>& insts, int precision, ResDe
   if (!sorted.empty())
     RGS_CUDA_TRY(cudaMemcpy(dev.work, sorted.data(), sorted.size() * sizeof(ResWork), cudaMemcpyHostToDevice));
   dev.nwork = (long long)sorted.size();
+  dev.variant = variant;
   return RGS_OK;
 }
 
@@ -491,7 +502,8 @@ int resident_launch(const ResDevice& dev, int precision, cudaStream_t stream, in
   if (dev.device < 0 || !dev.counter) return fail(RGS_ERR_ARG, "batch is not prepared");
   RGS_CUDA_TRY(cudaSetDevice(dev.device));
   RGS_CUDA_TRY(cudaMemsetAsync(dev.counter, 0, 2 * sizeof(int), stream));
-  const int blocks = (int)std::max<long long>(1, std::min<long long>(dev.nwork, sm_count(dev.device)));
+  const int per_sm = 512 / kResThreadsOf[dev.variant];
+  const int blocks = (int)std::max<long long>(1, std::min<long long>(dev.nwork, (long long)sm_count(dev.device) * per_sm));
   if (blocks_out) *blocks_out = dev.nwork ? blocks : 0;
   if (!dev.nwork) return RGS_OK;
   if (precision == RGS_PREC_C128) return launch_kernel<double, double>(dev, stream, blocks);

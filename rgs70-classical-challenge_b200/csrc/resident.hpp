@@ -12,9 +12,13 @@
 
 namespace rgs {
 
-constexpr int kResThreads = 512;              // threads per block (one block per SM)
 constexpr int kMaxResItems = 64;              // items of one work unit (a power of two)
-constexpr int kResidentSmem = 192 * 1024;     // dynamic shared memory per block: two tables
+// Launch variants: (threads per block, dynamic shared memory per block for the two tables)
+// -- one 512-thread block per SM with 192 KiB, or two 256-thread blocks with 94 KiB each
+// (more blocks to hide the per-position barriers; smaller tables).  rgs_batch_tune picks.
+constexpr int kResVariants = 2;
+constexpr int kResThreadsOf[kResVariants] = {512, 256};
+constexpr int kResSmemOf[kResVariants] = {192 * 1024, 94 * 1024};
 
 // One instance of a batch.  Device pointers; outputs of an unused kind may be null.
 struct ResInstance {
@@ -55,15 +59,17 @@ struct ResDevice {
   size_t work_cap = 0;
   int* counter = nullptr;  // [0]: next work unit, [1]: status (1 = a zero-mass branch pair)
   long long nwork = 0;
+  int variant = 0;         // launch variant the work list was prepared for
   ~ResDevice();
 };
 
-// Largest table rank the executor holds in shared memory for a precision.
-int resident_max_rank(int precision);
+// Largest table rank a launch variant holds in shared memory for a precision.
+int resident_max_rank(int precision, int variant = 0);
 // Items per work unit for an instance of rank `rmax` (0 if it does not fit).
-int resident_items(int rmax, int precision);
-// Uploads the instance records and the cost-ordered work list (synchronous).
-int resident_prepare(const std::vector<ResInstance>& insts, int precision, ResDevice& dev);
+int resident_items(int rmax, int precision, int variant = 0);
+// Sets every instance's items per unit for `variant`, uploads the instance records and
+// the cost-ordered work list (synchronous).
+int resident_prepare(const std::vector<ResInstance>& insts, int precision, int variant, ResDevice& dev);
 // Queues the persistent launch on `stream`: resets the work counter and status, then
 // runs every unit.  Capturable once prepared.
 int resident_launch(const ResDevice& dev, int precision, cudaStream_t stream, int* blocks_out);

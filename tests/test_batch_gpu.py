@@ -198,3 +198,26 @@ def test_errors(pkg):
     with pytest.raises(ValueError):
         rb.add(inst.g, inst.u[:5], inst.order, bits=np.zeros((2, 10), dtype=np.uint8))
     rb.run()  # an empty batch is a no-op
+
+
+def test_tuned_launch_variants(pkg):
+    """Both launch variants (one 512-thread block or two 256-thread blocks per SM) give the
+    streaming executor's amplitudes bit for bit; the tuner keeps one of them."""
+    insts = _instances(pkg, 10, 41, nlo=10, nhi=24, rmax=pkg.batch.max_rank("c64") - 1)
+    rng = np.random.default_rng(41)
+    rb = pkg.ResidentBatch("c64")
+    bits = []
+    for inst in insts:
+        b = pkg.instances.uniform_bits(int(rng.integers(1, 90)), inst.n, rng)
+        bits.append(b)
+        rb.add(inst.g, inst.u, inst.order, bits=b, nsamples=20, seed=5)
+    v, ms = rb.tune()
+    assert v in (0, 1) and ms[v] > 0
+    for variant_run in range(2):
+        rb.run()
+        for k, inst in enumerate(insts):
+            val, ls, _ = rb.amplitudes(k)
+            rv, rls = pkg.ScanOracle(inst.g, inst.u, inst.order).engine.sweep_bits(bits[k])
+            assert np.array_equal(val, rv) and np.array_equal(ls, rls)
+            sb, p, lp = rb.samples(k)
+            assert np.abs(lp - np.log(p)).max() < 1e-4
