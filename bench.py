@@ -672,7 +672,8 @@ def run_batched(args, rank, world, local_rank):
                                    f"{S} samples each per step, one persistent launch replayed from a CUDA graph",
                        "instances": nI, "strings_per_instance": K, "samples_per_instance": S,
                        "work_units": rb.units, "l2": "tables live in shared memory; HBM holds only inputs and outputs",
-                       "tuned_variant": {"chosen": ["512 threads, 1 block/SM", "256 threads, 2 blocks/SM"][variant],
+                       "tuned_variant": {"chosen": ["512 threads, 1 block/SM", "256 threads, 2 blocks/SM",
+                                                    "128 threads, 4 blocks/SM"][variant],
                                          "ms_per_run": tune_ms}},
             "roofline": {"bound": "smem", "achieved": tb * args.steps / t / 1e9, "peak": smem_peak, "unit": "GB/s",
                          "frac": tb * args.steps / t / 1e9 / smem_peak, "traffic": None,

@@ -177,10 +177,11 @@ int rgs_batch_info(const rgs_batch* batch, int32_t* instances, int64_t* units);
  * RGS_ERR_ZERO_NORM. */
 int rgs_batch_run(rgs_batch* batch, int32_t check, void* stream);
 /* Autotuning of the batch's launch: runs it with each launch variant that holds every
- * instance (one 512-thread block per SM with 192 KiB of tables, or two 256-thread blocks
- * with 94 KiB) and keeps the faster; *variant = the chosen one, ms[2] = milliseconds per
- * run (-1 where a variant does not fit; may be NULL).  Runs the batch (outputs are
- * written); synchronises.  No counterpart in the reference (it has no batch launch). */
+ * instance (one 512-thread block per SM with 192 KiB of tables, two 256-thread blocks with
+ * 94 KiB, or four 128-thread blocks with 44 KiB) and keeps the fastest; *variant = the
+ * chosen one, ms[3] = milliseconds per run (-1 where a variant does not fit; may be
+ * NULL).  Runs the batch (outputs are written); synchronises.  No counterpart in the
+ * reference (it has no batch launch). */
 int rgs_batch_tune(rgs_batch* batch, void* stream, int32_t* variant, float* ms);
 
 /* ---------------------------------------------------------------- conditional (Fourier-cut) sampler

@@ -135,11 +135,11 @@ class ResidentBatch:
         written).  Returns (variant, milliseconds per run of each variant)."""
         s = stream if stream is not None else torch.cuda.current_stream(self.device)
         v = ctypes.c_int32()
-        ms = (ctypes.c_float * 2)()
+        ms = (ctypes.c_float * 3)()
         with torch.cuda.device(self.device):
             _lib.check(_lib.lib().rgs_batch_tune(self._h, ctypes.c_void_p(s.cuda_stream), ctypes.byref(v), ms))
         self._graph = None
-        return int(v.value), [float(ms[0]), float(ms[1])]
+        return int(v.value), [float(x) for x in ms]
 
     def capture(self):
         """Captures ``run()`` into a CUDA graph (after a first, preparing run); returns it."""

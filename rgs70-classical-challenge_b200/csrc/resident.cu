@@ -415,7 +415,9 @@ int launch_variant(const ResDevice& dev, cudaStream_t stream, int blocks) {
 
 template <typename S, typename M>
 int launch_kernel(const ResDevice& dev, cudaStream_t stream, int blocks) {
-  return dev.variant ? launch_variant<S, M, 1>(dev, stream, blocks) : launch_variant<S, M, 0>(dev, stream, blocks);
+  if (dev.variant == 2) return launch_variant<S, M, 2>(dev, stream, blocks);
+  if (dev.variant == 1) return launch_variant<S, M, 1>(dev, stream, blocks);
+  return launch_variant<S, M, 0>(dev, stream, blocks);
 }
 
 size_t table_entries(int precision, int variant) {

@@ -14,11 +14,12 @@ namespace rgs {
 
 constexpr int kMaxResItems = 64;              // items of one work unit (a power of two)
 // Launch variants: (threads per block, dynamic shared memory per block for the two tables)
-// -- one 512-thread block per SM with 192 KiB, or two 256-thread blocks with 94 KiB each
-// (more blocks to hide the per-position barriers; smaller tables).  rgs_batch_tune picks.
-constexpr int kResVariants = 2;
-constexpr int kResThreadsOf[kResVariants] = {512, 256};
-constexpr int kResSmemOf[kResVariants] = {192 * 1024, 94 * 1024};
+// -- one 512-thread block per SM with 192 KiB, two 256-thread blocks with 94 KiB each, or
+// four 128-thread blocks with 44 KiB each (more blocks hide the per-position barriers;
+// smaller tables hold fewer items).  rgs_batch_tune picks.
+constexpr int kResVariants = 3;
+constexpr int kResThreadsOf[kResVariants] = {512, 256, 128};
+constexpr int kResSmemOf[kResVariants] = {192 * 1024, 94 * 1024, 44 * 1024};
 
 // One instance of a batch.  Device pointers; outputs of an unused kind may be null.
 struct ResInstance {

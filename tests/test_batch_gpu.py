@@ -212,7 +212,7 @@ def test_tuned_launch_variants(pkg):
         bits.append(b)
         rb.add(inst.g, inst.u, inst.order, bits=b, nsamples=20, seed=5)
     v, ms = rb.tune()
-    assert v in (0, 1) and ms[v] > 0
+    assert v in (0, 1, 2) and ms[v] > 0
     for variant_run in range(2):
         rb.run()
         for k, inst in enumerate(insts):
