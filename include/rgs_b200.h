@@ -97,10 +97,12 @@ int rgs_order_search(int32_t n, int32_t n_edges, const int32_t* edges, const int
  * with the same power-of-two renormalisation as the reference, computed on the
  * device (no per-step host round trip).
  *
- * Workspace: caller-owned device memory of at least
- * rgs_scan_workspace_bytes(plan, batch_tile, precision) bytes; batch_tile is a
- * power of two (1..rgs_scan_max_batch_tile) = bitstrings executed together in one
- * interleaved table. */
+ * Workspace: caller-owned device memory of rgs_scan_workspace_bytes(plan, batch_tile,
+ * precision) bytes; batch_tile is a power of two (1..rgs_scan_max_batch_tile) =
+ * bitstrings executed together in one interleaved table.  That size lets the sweep run
+ * chunks of 8192 bitstrings (several tiles) with one launch per low-rank position for the
+ * whole chunk; a smaller workspace (down to two tables of one tile) halves the chunk or,
+ * at the least, runs tile by tile, with the same results bit for bit. */
 int rgs_scan_workspace_bytes(const rgs_plan* plan, int32_t batch_tile, int32_t precision, size_t* bytes);
 /* Largest batch_tile accepted for a precision (128 complex64, 256 complex64/float32 math,
  * 64 complex128). */

@@ -176,10 +176,10 @@ int rgs_scan_max_batch_tile(int32_t precision, int32_t* tile) {
 
 int rgs_scan_workspace_bytes(const rgs_plan* plan, int32_t batch_tile, int32_t precision, size_t* bytes) {
   if (!plan || !bytes) return fail(RGS_ERR_ARG, "null argument");
-  ScanLayout L;
-  int rc = scan_layout(plan->plan, batch_tile, precision, L);
+  ChunkLayout C;
+  int rc = scan_chunk_layout(plan->plan, batch_tile, precision, scan_chunk_tiles(batch_tile), C);
   if (rc) return rc;
-  *bytes = L.total();
+  *bytes = C.total;
   return RGS_OK;
 }
 

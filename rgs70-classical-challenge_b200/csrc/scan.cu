@@ -181,6 +181,39 @@ __global__ void scan_finalize_kernel(const S* __restrict__ E, const u64* __restr
   out_logscale[b] = (double)esum * 0.69314718055994530942;
 }
 
+// The same over a chunk of tiles: item i is item i % Bt of tile i / Bt, whose final
+// table starts (i / Bt) * e_stride entries into E; maxima rows are `stride` items long.
+template <typename S>
+__global__ void scan_finalize_chunk_kernel(const S* __restrict__ E, u64 e_stride, int lbt,
+                                           const u64* __restrict__ maxbuf, int n, int stride, int count,
+                                           S* __restrict__ out_value, double* __restrict__ out_logscale) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  long long esum = 0;
+  bool zero = false, bad = false;
+  double m2prev = 1.0;
+  for (int j = 0; j < n; ++j) {
+    esum += scale_exponent(m2prev);
+    const double m2 = max_value<S>(maxbuf[(size_t)j * stride + i]);
+    if (!isfinite(m2)) {
+      bad = true;
+      break;
+    }
+    if (!(m2 > 0.0)) {
+      zero = true;
+      break;
+    }
+    m2prev = m2;
+  }
+  const u64 e = ((u64)(i >> lbt) * e_stride + (u64)(i & ((1 << lbt) - 1))) * 2;
+  S re = E[e], im = E[e + 1];
+  if (zero) re = im = (S)0;
+  if (bad) re = im = (S)NAN;
+  out_value[2 * (size_t)i] = re;
+  out_value[2 * (size_t)i + 1] = im;
+  out_logscale[i] = (double)esum * 0.69314718055994530942;
+}
+
 // ------------------------------------------------------------------------------------------------
 // Largest batch tile per precision: a lane owns at most 4 chunks (complex128: gathered
 // two at a time) or, with float32 arithmetic, 4 chunks of two items.
@@ -213,21 +246,68 @@ int scan_layout(const Plan& plan, int Bt, int precision, ScanLayout& L) {
   return RGS_OK;
 }
 
+// A chunk of S tiles whose small positions -- the leading and trailing positions whose
+// input and output ranks are at most kSmallRank -- run as one launch over all S tiles:
+// those tables are tiny, and one launch per tile and position would be launch-bound.  The
+// positions in between run tile by tile through two full-size tables as before.
+int scan_chunk_layout(const Plan& plan, int Bt, int precision, int S, ChunkLayout& L) {
+  ScanLayout base;
+  int rc = scan_layout(plan, Bt, precision, base);
+  if (rc) return rc;
+  if (S < 1) return fail(RGS_ERR_ARG, "chunk must hold at least one tile");
+  const int n = plan.n;
+  auto small = [&](int j) { return std::max(plan.steps[j].r_in, plan.steps[j].r_out) <= kSmallRank; };
+  int h = 0;
+  while (h < n && small(h)) ++h;
+  int t = n;
+  while (t > h && small(t - 1)) --t;
+  int rs = 0, rmid = 0;
+  for (int j = 0; j < n; ++j) {
+    const int r = std::max(plan.steps[j].r_in, plan.steps[j].r_out);
+    if (j < h || j >= t)
+      rs = std::max(rs, r);
+    else
+      rmid = std::max(rmid, r);
+  }
+  L.Bt = Bt;
+  L.S = S;
+  L.h = h;
+  L.t = t;
+  L.esize = base.esize;
+  L.e_stride = (unsigned long long)Bt << rs;
+  L.bytes_small = align_up((size_t)S * L.e_stride * L.esize, 256);
+  L.bytes_big = h < t ? align_up(((size_t)Bt << rmid) * L.esize, 256) : 0;
+  const size_t items = (size_t)S * Bt;
+  L.off_small0 = 0;
+  L.off_small1 = L.bytes_small;
+  L.off_big0 = 2 * L.bytes_small;
+  L.off_big1 = L.off_big0 + L.bytes_big;
+  L.off_w = L.off_big1 + L.bytes_big;
+  L.off_f = L.off_w + align_up((size_t)n * items * sizeof(double4), 256);
+  L.off_max = L.off_f + align_up((size_t)n * items, 256);
+  L.total = L.off_max + align_up((size_t)n * items * sizeof(u64), 256);
+  return RGS_OK;
+}
+
+int scan_chunk_tiles(int Bt) { return std::max(2, kChunkItems / Bt); }
+
 namespace {
 
 template <typename S, typename M, int VE, int CPL, int MODE, int NC, int NG0>
 cudaError_t launch_row(dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevStep& st, const u64* T,
-                       const double4* W, const unsigned char* F, const u64* mp, u64* mc, int lbt, int unit) {
+                       const double4* W, const unsigned char* F, const u64* mp, u64* mc, int lbt, int unit,
+                       u64 es) {
   scan_row_kernel<S, M, VE, MODE, NC, CPL, NG0><<<grid, 256, 0, s>>>((const S*)Ein, (S*)Eout, st, T, W, F, mp, mc,
-                                                                     lbt, unit);
+                                                                     lbt, unit, es);
   return cudaGetLastError();
 }
 
 template <typename S, typename M, int VE, int CPL>
 cudaError_t launch_modes(dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevStep& st, const u64* T,
-                         const double4* W, const unsigned char* F, const u64* mp, u64* mc, int lbt, int unit) {
+                         const double4* W, const unsigned char* F, const u64* mp, u64* mc, int lbt, int unit,
+                         u64 es) {
 #define RGS_ROW(MODE, NC, NG0) \
-  launch_row<S, M, VE, CPL, MODE, NC, NG0>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit)
+  launch_row<S, M, VE, CPL, MODE, NC, NG0>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit, es)
   if (st.mode == MODE_PAIR) {
     // The combos with kappa = 0 come first: all of them, or half (kappa is linear in the combo).
     if (st.ncombos == 1) return RGS_ROW(MODE_PAIR, 1, 1);
@@ -268,26 +348,30 @@ StepGeometry step_geometry(int precision, int Bt, const DevStep& st, int device)
   return g;
 }
 
+// One position over `tiles` tiles (grid.y) whose tables lie `es` entries apart.
 cudaError_t launch_step(int precision, int Bt, int device, cudaStream_t s, const void* Ein, void* Eout,
                         const DevStep& st, const u64* T, const double4* W, const unsigned char* F, const u64* mp,
-                        u64* mc, int unit) {
+                        u64* mc, int unit, int tiles = 1, u64 es = 0) {
   const StepGeometry g = step_geometry(precision, Bt, st, device);
   const int lbt = __builtin_ctz((unsigned)Bt);
-  const dim3 grid((unsigned)g.blocks);
+  const dim3 grid((unsigned)g.blocks, (unsigned)tiles);
+#define RGS_MODES(S_, M_, VE_, CPL_) \
+  launch_modes<S_, M_, VE_, CPL_>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit, es)
   if (precision == RGS_PREC_C128) {
-    if (g.CPL == 1) return launch_modes<double, double, 1, 1>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
-    if (g.CPL == 2) return launch_modes<double, double, 1, 2>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
-    return launch_modes<double, double, 1, 4>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+    if (g.CPL == 1) return RGS_MODES(double, double, 1, 1);
+    if (g.CPL == 2) return RGS_MODES(double, double, 1, 2);
+    return RGS_MODES(double, double, 1, 4);
   }
   if (precision == RGS_PREC_C64) {
-    if (g.VE == 1) return launch_modes<float, double, 1, 1>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
-    if (g.CPL == 1) return launch_modes<float, double, 2, 1>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
-    return launch_modes<float, double, 2, 2>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+    if (g.VE == 1) return RGS_MODES(float, double, 1, 1);
+    if (g.CPL == 1) return RGS_MODES(float, double, 2, 1);
+    return RGS_MODES(float, double, 2, 2);
   }
-  if (g.VE == 1) return launch_modes<float, float, 1, 1>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
-  if (g.CPL == 1) return launch_modes<float, float, 2, 1>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
-  if (g.CPL == 2) return launch_modes<float, float, 2, 2>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
-  return launch_modes<float, float, 2, 4>(grid, s, Ein, Eout, st, T, W, F, mp, mc, lbt, unit);
+  if (g.VE == 1) return RGS_MODES(float, float, 1, 1);
+  if (g.CPL == 1) return RGS_MODES(float, float, 2, 1);
+  if (g.CPL == 2) return RGS_MODES(float, float, 2, 2);
+  return RGS_MODES(float, float, 2, 4);
+#undef RGS_MODES
 }
 
 bool plan_has_fixed(const Plan& p) {
@@ -298,9 +382,13 @@ bool plan_has_fixed(const Plan& p) {
 
 }  // namespace
 
-int scan_run(Plan& plan, const double* U, const u64* bits, const double* fvec, long long batch, int precision,
-             void* out_value, double* out_logscale, void* workspace, size_t ws_bytes, int Bt, cudaStream_t stream,
-             ScanStats* stats) {
+namespace {
+
+// Tile-by-tile sweep (every position, one launch per tile): the path for workspaces sized
+// by scan_layout alone.
+int scan_run_tiles(Plan& plan, const double* U, const u64* bits, const double* fvec, long long batch, int precision,
+                   void* out_value, double* out_logscale, void* workspace, size_t ws_bytes, int Bt,
+                   cudaStream_t stream, ScanStats* stats) {
   if (batch < 0) return fail(RGS_ERR_ARG, "batch must be >= 0");
   if (batch == 0) return RGS_OK;
   if (!out_value || !out_logscale || !workspace) return fail(RGS_ERR_ARG, "null output or workspace pointer");
@@ -308,7 +396,7 @@ int scan_run(Plan& plan, const double* U, const u64* bits, const double* fvec, l
   ScanLayout L;
   int rc = scan_layout(plan, Bt, precision, L);
   if (rc) return rc;
-  if (ws_bytes < L.total()) return fail(RGS_ERR_OOM, "workspace smaller than rgs_scan_workspace_bytes()");
+  if (ws_bytes < L.total()) return fail(RGS_ERR_OOM, "workspace smaller than one tile's layout (rgs_scan_workspace_bytes)");
   if (((uintptr_t)workspace & 255) != 0) return fail(RGS_ERR_ARG, "workspace must be 256-byte aligned");
   int device = 0;
   rc = bind_device_of(workspace, &device);
@@ -348,6 +436,128 @@ int scan_run(Plan& plan, const double* U, const u64* bits, const double* fvec, l
           (const float*)fin, maxbuf, plan.n, Bt, count, (float*)out_value + 2 * first, out_logscale + first);
     RGS_CUDA_TRY(cudaGetLastError());
     launches += 1;
+  }
+  if (stats) stats->launches = launches;
+  return RGS_OK;
+}
+
+}  // namespace
+
+int scan_run(Plan& plan, const double* U, const u64* bits, const double* fvec, long long batch, int precision,
+             void* out_value, double* out_logscale, void* workspace, size_t ws_bytes, int Bt, cudaStream_t stream,
+             ScanStats* stats) {
+  if (batch < 0) return fail(RGS_ERR_ARG, "batch must be >= 0");
+  if (batch == 0) return RGS_OK;
+  if (!out_value || !out_logscale || !workspace) return fail(RGS_ERR_ARG, "null output or workspace pointer");
+  if (!fvec && (!U || !bits)) return fail(RGS_ERR_ARG, "need unitaries and bits, or contraction vectors");
+  ScanLayout L;
+  int rc = scan_layout(plan, Bt, precision, L);
+  if (rc) return rc;
+  // The largest chunk of tiles the workspace holds; a workspace sized by scan_layout alone
+  // runs tile by tile.
+  ChunkLayout C;
+  int S = scan_chunk_tiles(Bt);
+  while (S >= 2) {
+    if ((rc = scan_chunk_layout(plan, Bt, precision, S, C))) return rc;
+    if (C.total <= ws_bytes) break;
+    S >>= 1;
+  }
+  if (S < 2)
+    return scan_run_tiles(plan, U, bits, fvec, batch, precision, out_value, out_logscale, workspace, ws_bytes, Bt,
+                          stream, stats);
+  if (((uintptr_t)workspace & 255) != 0) return fail(RGS_ERR_ARG, "workspace must be 256-byte aligned");
+  int device = 0;
+  rc = bind_device_of(workspace, &device);
+  if (rc) return rc;
+  const Plan::DeviceCopy* dc = nullptr;
+  rc = plan_device_copy(plan, device, &dc);
+  if (rc) return rc;
+
+  const int n = plan.n, h = C.h, t = C.t;
+  const int stride = S * Bt;  // items per row of the weights, flags and maxima
+  const size_t esize = C.esize;
+  char* ws = (char*)workspace;
+  char* small[2] = {ws + C.off_small0, ws + C.off_small1};
+  char* big[2] = {ws + C.off_big0, ws + C.off_big1};
+  double4* W = (double4*)(ws + C.off_w);
+  unsigned char* F = plan_has_fixed(plan) ? (unsigned char*)(ws + C.off_f) : nullptr;
+  u64* maxbuf = (u64*)(ws + C.off_max);
+  const u64* tables = (const u64*)dc->tables;
+  const int lbt = __builtin_ctz((unsigned)Bt);
+  long long launches = 0;
+  auto wrow = [&](int j) { return W + (size_t)j * stride; };
+  auto frow = [&](int j) { return F ? F + (size_t)j * stride : nullptr; };
+  auto mrow = [&](int j) { return maxbuf + (size_t)j * stride; };
+
+  for (long long first = 0; first < batch; first += stride) {
+    const int count = (int)std::min<long long>(stride, batch - first);
+    const int tiles = (count + Bt - 1) / Bt;
+    scan_weights_kernel<<<(stride + 127) / 128, 128, 0, stream>>>((const DevVert*)dc->verts, n, (const double2*)U,
+                                                                  bits, (const double2*)fvec, first, count, stride, W,
+                                                                  F);
+    RGS_CUDA_TRY(cudaGetLastError());
+    RGS_CUDA_TRY(cudaMemsetAsync(maxbuf, 0, (size_t)n * stride * sizeof(u64), stream));
+    launches += 1;
+    int cur = 0;
+    // Leading small positions: all tiles of the chunk per launch.
+    for (int j = 0; j < h; ++j) {
+      const DevStep& st = plan.dev[j];
+      RGS_CUDA_TRY(launch_step(precision, Bt, device, stream, small[cur], small[cur ^ 1], st, tables + st.table_off,
+                               wrow(j), frow(j), j ? mrow(j - 1) : nullptr, mrow(j), j == 0, tiles, C.e_stride));
+      cur ^= 1;
+      launches += 1;
+    }
+    // Middle positions, tile by tile: from the tile's slice of the small buffer through the
+    // full-size tables to its slice of the other small buffer (or to the final value).
+    if (h < t) {
+      for (int k = 0; k < tiles; ++k) {
+        const size_t koff = (size_t)k * C.e_stride * esize;
+        for (int j = h; j < t; ++j) {
+          const DevStep& st = plan.dev[j];
+          const void* in = j == h ? (const void*)(small[cur] + koff) : (const void*)big[(j - h) & 1];
+          void* out = (j == t - 1 && t < n) ? (void*)(small[cur ^ 1] + koff) : (void*)big[(j - h + 1) & 1];
+          RGS_CUDA_TRY(launch_step(precision, Bt, device, stream, in, out, st, tables + st.table_off,
+                                   wrow(j) + (size_t)k * Bt, frow(j) ? frow(j) + (size_t)k * Bt : nullptr,
+                                   j ? mrow(j - 1) + (size_t)k * Bt : nullptr, mrow(j) + (size_t)k * Bt, j == 0));
+          launches += 1;
+        }
+        if (t == n) {  // the sweep ends in the full-size tables: finalise this tile now
+          const int kc = std::min(Bt, count - k * Bt);
+          const void* fin = big[(t - h) & 1];
+          if (precision == RGS_PREC_C128)
+            scan_finalize_chunk_kernel<double><<<(kc + 127) / 128, 128, 0, stream>>>(
+                (const double*)fin, 0ull, lbt, maxbuf + (size_t)k * Bt, n, stride, kc,
+                (double*)out_value + 2 * (first + (long long)k * Bt), out_logscale + first + (long long)k * Bt);
+          else
+            scan_finalize_chunk_kernel<float><<<(kc + 127) / 128, 128, 0, stream>>>(
+                (const float*)fin, 0ull, lbt, maxbuf + (size_t)k * Bt, n, stride, kc,
+                (float*)out_value + 2 * (first + (long long)k * Bt), out_logscale + first + (long long)k * Bt);
+          RGS_CUDA_TRY(cudaGetLastError());
+          launches += 1;
+        }
+      }
+      if (t < n) cur ^= 1;
+    }
+    // Trailing small positions: all tiles per launch again.
+    if (t < n || h == n) {
+      for (int j = std::max(t, h); j < n; ++j) {
+        const DevStep& st = plan.dev[j];
+        RGS_CUDA_TRY(launch_step(precision, Bt, device, stream, small[cur], small[cur ^ 1], st, tables + st.table_off,
+                                 wrow(j), frow(j), j ? mrow(j - 1) : nullptr, mrow(j), j == 0, tiles, C.e_stride));
+        cur ^= 1;
+        launches += 1;
+      }
+      if (precision == RGS_PREC_C128)
+        scan_finalize_chunk_kernel<double><<<(count + 127) / 128, 128, 0, stream>>>(
+            (const double*)small[cur], C.e_stride, lbt, maxbuf, n, stride, count, (double*)out_value + 2 * first,
+            out_logscale + first);
+      else
+        scan_finalize_chunk_kernel<float><<<(count + 127) / 128, 128, 0, stream>>>(
+            (const float*)small[cur], C.e_stride, lbt, maxbuf, n, stride, count, (float*)out_value + 2 * first,
+            out_logscale + first);
+      RGS_CUDA_TRY(cudaGetLastError());
+      launches += 1;
+    }
   }
   if (stats) stats->launches = launches;
   return RGS_OK;

@@ -24,6 +24,22 @@ struct ScanStats {
 
 int scan_layout(const Plan& plan, int Bt, int precision, ScanLayout& L);
 
+// Chunked sweep (scan_run): S tiles share one launch per small position (input and output
+// rank at most kSmallRank); the positions between the leading and trailing small ones
+// (h <= j < t) run tile by tile.  Workspace: two small-table buffers of S tiles, two
+// full-size tables for the middle positions, weights / flags / maxima of S tiles.
+constexpr int kSmallRank = 12;
+constexpr int kChunkItems = 8192;  // default items per chunk (S = kChunkItems / Bt tiles)
+struct ChunkLayout {
+  int Bt = 1, S = 1, h = 0, t = 0;
+  size_t esize = 8;
+  unsigned long long e_stride = 0;  // entries per tile in the small buffers
+  size_t bytes_small = 0, bytes_big = 0;
+  size_t off_small0 = 0, off_small1 = 0, off_big0 = 0, off_big1 = 0, off_w = 0, off_f = 0, off_max = 0, total = 0;
+};
+int scan_chunk_layout(const Plan& plan, int Bt, int precision, int S, ChunkLayout& L);
+int scan_chunk_tiles(int Bt);
+
 // Largest batch tile the step kernel supports for a precision.
 int scan_max_tile(int precision);
 

@@ -1,5 +1,6 @@
-// Streaming scan-step kernel: one scan position over a batch tile, rows of the
-// interleaved table handled by (sub-)warps.
+// Streaming scan-step kernel: one scan position over a batch tile (or, along grid.y,
+// several tiles whose tables lie e_stride entries apart), rows of the interleaved table
+// handled by (sub-)warps.
 //
 // A row of Bt items is 2^lC chunks of 16 bytes.  L = min(32, 2^lC) lanes share a row
 // and each lane owns CPL chunks (CPL = 2^lC / L), so the row's gather index (byte-table
@@ -61,7 +62,7 @@ __global__ void __launch_bounds__(256, 2) scan_row_kernel(const S* __restrict__ 
                                                        const u64* __restrict__ T, const double4* __restrict__ W,
                                                        const unsigned char* __restrict__ F,
                                                        const u64* __restrict__ maxprev, u64* __restrict__ maxcur,
-                                                       int lbt, int unit_input) {
+                                                       int lbt, int unit_input, u64 e_stride) {
   constexpr int CPLG = ChunkGroup<S, M, CPL>::value;
   constexpr int U = RowsPerIter<NC, CPLG, LoadsInFlight<S, M>::value>::value;
   constexpr int NI = CPL * VE;             // items owned by a lane
@@ -74,6 +75,17 @@ __global__ void __launch_bounds__(256, 2) scan_row_kernel(const S* __restrict__ 
   const int sub = lane >> lL;
   const int l = lane & ((1 << lL) - 1);
 
+  // Several tiles in one launch (grid.y): tile k's table starts k * e_stride entries in,
+  // its weights, flags and maxima k * Bt items in.
+  if (blockIdx.y) {
+    const u64 k = blockIdx.y;
+    Ein += 2 * k * e_stride;
+    Eout += 2 * k * e_stride;
+    W += k << lbt;
+    if (F) F += k << lbt;
+    if (maxprev) maxprev += k << lbt;
+    maxcur += k << lbt;
+  }
   for (int i = threadIdx.x; i < Bt; i += blockDim.x) smax[i] = 0;
 
   Cx<M> wA[NI], wB[NI];
