@@ -219,7 +219,7 @@ def run_ours(args, rank, world, local_rank):
             eng128.run_bits(d_bits, v128, l128, stream=s)
 
     # One sweep eagerly (allocates the workspaces), then the step as a CUDA graph: the
-    # 42 launches per tile replay without host launch overhead.
+    # sweep's launches replay without host launch overhead.
     queue_step(stream)
     torch.cuda.synchronize(device)
     tile64 = eng64.batch_tile if use64 else None
@@ -323,7 +323,8 @@ def run_ours(args, rank, world, local_rank):
     h2d = packed.nbytes
     d2h = BATCH * ((8 + 8 if use64 else 0) + (16 + 8 if use128 else 0))
 
-    # Roofline of the scan-step kernels (dominant: they are all but three launches per tile).
+    # Roofline of the scan-step kernels (dominant: every launch but the weights and
+    # finalisation kernels, one or two per chunk of tiles).
     b64 = step_bytes(inst.ranks, 8) * BATCH if use64 else 0
     b128 = step_bytes(inst.ranks, 16) * BATCH if use128 else 0
     peaks_path = ROOT / "MEASURED_PEAKS.json"
@@ -331,19 +332,19 @@ def run_ours(args, rank, world, local_rank):
     if peaks_path.exists():
         peak, peak_src = float(json.loads(peaks_path.read_text())["hbm_gbs"]), "measured"
     achieved = (b64 + b128) / (t_step / args.steps) / 1e9
-    # DRAM traffic of one tile sweep from one ncu capture, times the tiles of this step
-    # (valid for the tile sizes it was captured at).
+    # DRAM traffic of one chunk sweep (8192 strings) from one ncu capture, times the chunks
+    # of this step (valid for the tile sizes it was captured at).
     traffic = None
     traffic_path = ROOT / "profiles" / "scan_step_traffic.json"
     if traffic_path.exists():
-        tr = json.loads(traffic_path.read_text())["dram_bytes_per_tile"]
+        tr = json.loads(traffic_path.read_text()).get("dram_bytes_per_chunk", {})
         t64r, t128r = tr.get(args.bulk), tr.get("c128")
         if (not use64 or (t64r and t64r["tile"] == tile64)) and (not use128 or (t128r and t128r["tile"] == tile128)):
-            traffic = ((math.ceil(BATCH / tile64) * t64r["bytes"] if use64 else 0)
-                       + (math.ceil(BATCH / tile128) * t128r["bytes"] if use128 else 0))
-    groups64 = math.ceil(BATCH / tile64) if use64 else 0
-    groups128 = math.ceil(BATCH / tile128) if use128 else 0
-    launches = args.steps * ((groups64 + groups128) * (N_QUBITS + 2))
+            traffic = ((BATCH / t64r["items"] * t64r["bytes"] if use64 else 0)
+                       + (BATCH / t128r["items"] * t128r["bytes"] if use128 else 0))
+    # Kernel launches of one step, from the library's own schedule.
+    launches = args.steps * ((eng64.launch_count(BATCH) if use64 else 0)
+                             + (eng128.launch_count(BATCH) if use128 else 0))
 
     # Secondary: exact Born samples/s of the chain sampler on the same instance.
     saved = BATCH
@@ -746,7 +747,8 @@ def run_rgs70(args, rank, world, local_rank):
             esize = 16 if prec == "c128" else 8
             legs[prec] = {"amplitudes_per_s": len(bits) * args.steps / t, "batch_tile": tile,
                           "max_rel_err_vs_reference_c128": float(np.max(np.abs(p - ref_p) / ref_p)),
-                          "achieved_GBps": step_bytes(plan_f.ranks, esize) * len(bits) * args.steps / t / 1e9}
+                          "achieved_GBps": step_bytes(plan_f.ranks, esize) * len(bits) * args.steps / t / 1e9,
+                          "launches_per_sweep": eng.launch_count(len(bits))}
             del eng, val, ls
             free()
         # Exact Born samples, complex64 tables, 8 samples per tile: the reference's optimised
@@ -809,7 +811,7 @@ def run_rgs70(args, rank, world, local_rank):
                                     "c128_amplitudes_per_s_1xH200": RGS70_REF_C128_AMP_PER_S,
                                     "born_samples_per_s_2xH200": RGS70_REF_SAMPLES_PER_S_2GPU},
             "exact_born_samples": samples_out,
-            "gpu_launches": args.steps * -(-len(bits) // 8) * (70 + 2), "clocks": clocks.summary()}
+            "gpu_launches": args.steps * legs["c64"]["launches_per_sweep"], "clocks": clocks.summary()}
     if rank == 0:
         print(json.dumps(line), flush=True)
 

@@ -107,6 +107,11 @@ int rgs_scan_workspace_bytes(const rgs_plan* plan, int32_t batch_tile, int32_t p
 /* Largest batch_tile accepted for a precision (128 complex64, 256 complex64/float32 math,
  * 64 complex128). */
 int rgs_scan_max_batch_tile(int32_t precision, int32_t* tile);
+/* Kernel launches rgs_scan_amplitudes / rgs_scan_contract queue for `batch` items with a
+ * workspace of workspace_bytes (host only, no GPU needed).  No reference counterpart: it
+ * reports the launch schedule for profiling and launch-count accounting. */
+int rgs_scan_launch_count(const rgs_plan* plan, int64_t batch, int32_t batch_tile, int32_t precision,
+                          size_t workspace_bytes, int64_t* launches);
 
 /* Bitstring interface: f_q = U_q[x_q, :] (W/scan_oracle.py:26).
  * unitaries: device complex128[n][2][2]; bits: device uint64[batch][2];

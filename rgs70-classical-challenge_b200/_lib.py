@@ -59,6 +59,8 @@ SIGNATURES = {
     "rgs_rank_profile": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p, c_uint8_p,
                                         c_int32_p]),
     "rgs_scan_workspace_bytes": (ctypes.c_int, [c_void_p, ctypes.c_int32, ctypes.c_int32, c_size_t_p]),
+    "rgs_scan_launch_count": (ctypes.c_int, [c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
+                                             ctypes.c_size_t, ctypes.POINTER(ctypes.c_int64)]),
     "rgs_order_search": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p, ctypes.c_int32,
                                         ctypes.c_int64, ctypes.c_uint64, ctypes.c_int32, c_int32_p, c_int32_p,
                                         c_double_p]),

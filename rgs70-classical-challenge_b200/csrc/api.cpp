@@ -203,6 +203,16 @@ int rgs_scan_contract(rgs_plan* plan, const double* fvec, int64_t batch, int32_t
                   workspace_bytes, batch_tile, (cudaStream_t)stream, nullptr);
 }
 
+int rgs_scan_launch_count(const rgs_plan* plan, int64_t batch, int32_t batch_tile, int32_t precision,
+                          size_t workspace_bytes, int64_t* launches) {
+  if (!plan || !launches) return fail(RGS_ERR_ARG, "null argument");
+  long long c = 0;
+  int rc = scan_launch_count(plan->plan, batch, batch_tile, precision, workspace_bytes, &c);
+  if (rc) return rc;
+  *launches = c;
+  return RGS_OK;
+}
+
 int rgs_chain_workspace_bytes(const rgs_plan* plan, int32_t batch_tile, int32_t precision, size_t* bytes) {
   if (!plan || !bytes) return fail(RGS_ERR_ARG, "null argument");
   ChainLayout L;

@@ -382,6 +382,44 @@ bool plan_has_fixed(const Plan& p) {
 
 }  // namespace
 
+int scan_pick_chunk(const Plan& plan, int Bt, int precision, size_t ws_bytes, ChunkLayout& C, int* S_out) {
+  *S_out = 0;
+  for (int S = scan_chunk_tiles(Bt); S >= 2; S >>= 1) {
+    int rc = scan_chunk_layout(plan, Bt, precision, S, C);
+    if (rc) return rc;
+    if (C.total <= ws_bytes) {
+      *S_out = S;
+      return RGS_OK;
+    }
+  }
+  return RGS_OK;
+}
+
+int scan_launch_count(const Plan& plan, long long batch, int Bt, int precision, size_t ws_bytes, long long* out) {
+  if (batch < 0) return fail(RGS_ERR_ARG, "batch must be >= 0");
+  ScanLayout L;
+  int rc = scan_layout(plan, Bt, precision, L);
+  if (rc) return rc;
+  ChunkLayout C;
+  int S = 0;
+  if ((rc = scan_pick_chunk(plan, Bt, precision, ws_bytes, C, &S))) return rc;
+  const long long n = plan.n;
+  long long total = 0;
+  if (S < 2) {
+    total = (batch + Bt - 1) / Bt * (n + 2);
+  } else {
+    const long long stride = (long long)S * Bt;
+    for (long long first = 0; first < batch; first += stride) {
+      const long long tiles = (std::min(stride, batch - first) + Bt - 1) / Bt;
+      total += 1 + C.h;
+      if (C.h < C.t) total += tiles * (C.t - C.h) + (C.t == n ? tiles : 0);
+      if (C.t < n || C.h == n) total += n - std::max(C.t, C.h) + 1;
+    }
+  }
+  *out = total;
+  return RGS_OK;
+}
+
 namespace {
 
 // Tile-by-tile sweep (every position, one launch per tile): the path for workspaces sized
@@ -450,18 +488,10 @@ int scan_run(Plan& plan, const double* U, const u64* bits, const double* fvec, l
   if (batch == 0) return RGS_OK;
   if (!out_value || !out_logscale || !workspace) return fail(RGS_ERR_ARG, "null output or workspace pointer");
   if (!fvec && (!U || !bits)) return fail(RGS_ERR_ARG, "need unitaries and bits, or contraction vectors");
-  ScanLayout L;
-  int rc = scan_layout(plan, Bt, precision, L);
-  if (rc) return rc;
-  // The largest chunk of tiles the workspace holds; a workspace sized by scan_layout alone
-  // runs tile by tile.
   ChunkLayout C;
-  int S = scan_chunk_tiles(Bt);
-  while (S >= 2) {
-    if ((rc = scan_chunk_layout(plan, Bt, precision, S, C))) return rc;
-    if (C.total <= ws_bytes) break;
-    S >>= 1;
-  }
+  int S = 0;
+  int rc = scan_pick_chunk(plan, Bt, precision, ws_bytes, C, &S);
+  if (rc) return rc;
   if (S < 2)
     return scan_run_tiles(plan, U, bits, fvec, batch, precision, out_value, out_logscale, workspace, ws_bytes, Bt,
                           stream, stats);

@@ -39,6 +39,11 @@ struct ChunkLayout {
 };
 int scan_chunk_layout(const Plan& plan, int Bt, int precision, int S, ChunkLayout& L);
 int scan_chunk_tiles(int Bt);
+// Tiles per chunk that scan_run uses with a workspace of ws_bytes (the largest S <=
+// scan_chunk_tiles(Bt), S >= 2, whose layout fits, with C filled in); 0: tile by tile.
+int scan_pick_chunk(const Plan& plan, int Bt, int precision, size_t ws_bytes, ChunkLayout& C, int* S);
+// Kernel launches scan_run queues for `batch` items with that workspace.
+int scan_launch_count(const Plan& plan, long long batch, int Bt, int precision, size_t ws_bytes, long long* out);
 
 // Largest batch tile the step kernel supports for a precision.
 int scan_max_tile(int precision);

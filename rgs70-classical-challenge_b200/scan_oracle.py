@@ -162,6 +162,16 @@ class ScanEngine:
                                                        ctypes.byref(nb)))
         return int(nb.value)
 
+    def launch_count(self, batch, tile=None):
+        """Kernel launches of one sweep of ``batch`` items (with the workspace this engine
+        allocates for ``tile``, default: the tile in use)."""
+        tile = int(tile or self._ws_tile or self.tile_for(batch))
+        ws = self._ws.numel() if self._ws is not None and self._ws_tile == tile else self.workspace_bytes(tile)
+        out = ctypes.c_int64()
+        _lib.check(_lib.lib().rgs_scan_launch_count(self.plan.handle, int(batch), tile, self.prec_code, ws,
+                                                    ctypes.byref(out)))
+        return int(out.value)
+
     def workspace(self, tile):
         need = self.workspace_bytes(tile)
         if self._ws is None or self._ws.numel() < need:

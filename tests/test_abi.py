@@ -46,3 +46,45 @@ def test_product_path_does_not_import_oracle():
     for py in pkg_dir.rglob("*.py"):
         src = py.read_text()
         assert "import oracle" not in src and "from oracle" not in src, py
+
+
+def _launches(pkg, plan, batch, tile, prec, ws):
+    out = ctypes.c_int64()
+    pkg._lib.check(pkg._lib.lib().rgs_scan_launch_count(plan.handle, batch, tile, prec, ws, ctypes.byref(out)))
+    return out.value
+
+
+def test_scan_launch_schedule(pkg):
+    """Launch count of a sweep: with the full workspace, the low-rank leading and trailing
+    positions run once per chunk of tiles; with a one-tile workspace, every position runs
+    once per tile (n steps + weights + finalisation)."""
+    inst = pkg.instances.make_instance("reg3", 40, 40, pkg.rank_profile)
+    plan = pkg.ScanPlan(inst.n, pkg.edges_from_graph(inst.g), inst.order)
+    n, ranks = inst.n, list(plan.ranks)
+    r_in = [0] + ranks[:-1]
+    small = [max(a, b) <= 12 for a, b in zip(r_in, ranks)]
+    h = 0
+    while h < n and small[h]:
+        h += 1
+    t = n
+    while t > h and small[t - 1]:
+        t -= 1
+    prec = pkg._lib.PREC_C64_F32
+    for tile in (8, 64, 256):
+        ws = ctypes.c_size_t()
+        pkg._lib.check(pkg._lib.lib().rgs_scan_workspace_bytes(plan.handle, tile, prec, ctypes.byref(ws)))
+        chunk = max(2, 8192 // tile) * tile
+        for batch in (1, tile, chunk, 3 * chunk + 5):
+            expect = 0
+            for first in range(0, batch, chunk):
+                tiles = -(-min(chunk, batch - first) // tile)
+                expect += 1 + h
+                if h < t:
+                    expect += tiles * (t - h) + (tiles if t == n else 0)
+                if t < n or h == n:
+                    expect += n - max(t, h) + 1
+            assert _launches(pkg, plan, batch, tile, prec, ws.value) == expect, (tile, batch)
+        # One tile's tables only: the tile-by-tile schedule.
+        per_tile = 2 * ((tile << max(ranks)) * 8) + n * tile * (32 + 1 + 8)
+        got = _launches(pkg, plan, 1000, tile, prec, per_tile + 4096)
+        assert got == -(-1000 // tile) * (n + 2)
