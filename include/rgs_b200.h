@@ -74,6 +74,29 @@ int rgs_plan_step(const rgs_plan* plan, int32_t j, int32_t* v, int32_t* is_free,
 /* Byte tables of step j (byte_tables, scan_plan.py:133-145): uint64[nbytes][256][2]
  * (lo, hi); pass tables = NULL to query nbytes. */
 int rgs_plan_step_tables(const rgs_plan* plan, int32_t j, uint64_t* tables, int32_t* nbytes);
+
+/* Fused pairs (no reference counterpart: an execution choice of this engine).  The
+ * compiler runs chosen consecutive free positions j, j + 1 of plans without fixed
+ * vertices as one pass (scan_pair_kernel) that keeps the table between them out of
+ * memory, choosing non-overlapping pairs that keep the most entries out of HBM.
+ * rgs_plan_set_fusion(plan, 0) turns this off, (…, 1) back on; only before the plan's
+ * first use on a device (RGS_ERR_ARG after).  Amplitudes agree to rounding either way;
+ * a (value, logscale) pair of the two schedules may differ by an exact power of two. */
+int rgs_plan_set_fusion(rgs_plan* plan, int32_t on);
+/* Number of fused pairs and (if first_positions is not NULL) position j of each,
+ * int32[count]. */
+int rgs_plan_pairs(const rgs_plan* plan, int32_t* count, int32_t* first_positions);
+/* Pair record k for inspection: the GF(2) data the pair kernel runs on.  Codes:
+ * 0 PAIR 1 combo, 1 PAIR 2 combos (second with y bit 1), 2 PAIR 2 combos (both y bit 0),
+ * 3 PAIR 4 combos (two with y bit 1), 4 MERGE 2 combos. */
+typedef struct rgs_pair_info {
+  int32_t j, code_a, code_b, a, m, o, dw, piv[3];
+  uint32_t pw_b;
+  uint64_t mask_a, beta_a, comb_a[4], la_w[4], beta_b, mb0[2], t_b;
+  uint64_t la_cols[64]; /* L_A: intermediate bit i -> A input vector (y bit at a), i < m */
+  uint64_t mb_cols[64]; /* M_B: intermediate bit i -> output row, i < m */
+} rgs_pair_info;
+int rgs_plan_pair_info(const rgs_plan* plan, int32_t k, rgs_pair_info* info);
 /* Rank profile without keeping a plan (cost model sum 2^r used by order search). */
 int rgs_rank_profile(int32_t n, int32_t n_edges, const int32_t* edges, const int32_t* order,
                      const uint8_t* fixed, int32_t* ranks);

@@ -8,7 +8,8 @@ sm_100a CUDA kernels in ``librgs_b200.so`` through the C ABI of
 from . import _lib
 from .plan import ScanPlan, Step, make_plan, future_masks, rank_profile, byte_tables, kernel_combos, \
     edges_from_graph, search_order
-from .scan_oracle import ScanEngine, ScanOracle, pack_bits, amplitudes_from, PRECISIONS, capture_graph, autotune_tile
+from .scan_oracle import ScanEngine, ScanOracle, pack_bits, amplitudes_from, PRECISIONS, capture_graph, autotune_tile, \
+    max_batch_tile
 from . import instances
 from .samplers import ConditionalSampler, DrawRecorder, produce, fwht, product, block_mass
 from .chain import ChainSampler, unpack_bits

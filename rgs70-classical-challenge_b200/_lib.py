@@ -36,6 +36,16 @@ _EXC = {
 }
 
 c_int32_p = ctypes.POINTER(ctypes.c_int32)
+
+
+class PairInfo(ctypes.Structure):
+    """``rgs_pair_info`` of include/rgs_b200.h."""
+    _fields_ = [("j", ctypes.c_int32), ("code_a", ctypes.c_int32), ("code_b", ctypes.c_int32),
+                ("a", ctypes.c_int32), ("m", ctypes.c_int32), ("o", ctypes.c_int32), ("dw", ctypes.c_int32),
+                ("piv", ctypes.c_int32 * 3), ("pw_b", ctypes.c_uint32),
+                ("mask_a", ctypes.c_uint64), ("beta_a", ctypes.c_uint64), ("comb_a", ctypes.c_uint64 * 4),
+                ("la_w", ctypes.c_uint64 * 4), ("beta_b", ctypes.c_uint64), ("mb0", ctypes.c_uint64 * 2),
+                ("t_b", ctypes.c_uint64), ("la_cols", ctypes.c_uint64 * 64), ("mb_cols", ctypes.c_uint64 * 64)]
 c_uint64_p = ctypes.POINTER(ctypes.c_uint64)
 c_uint8_p = ctypes.POINTER(ctypes.c_uint8)
 c_double_p = ctypes.POINTER(ctypes.c_double)
@@ -58,6 +68,9 @@ SIGNATURES = {
     "rgs_plan_step_tables": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_uint64_p, c_int32_p]),
     "rgs_rank_profile": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p, c_uint8_p,
                                         c_int32_p]),
+    "rgs_plan_set_fusion": (ctypes.c_int, [c_void_p, ctypes.c_int32]),
+    "rgs_plan_pairs": (ctypes.c_int, [c_void_p, c_int32_p, c_int32_p]),
+    "rgs_plan_pair_info": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_void_p]),
     "rgs_scan_workspace_bytes": (ctypes.c_int, [c_void_p, ctypes.c_int32, ctypes.c_int32, c_size_t_p]),
     "rgs_scan_launch_count": (ctypes.c_int, [c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
                                              ctypes.c_size_t, ctypes.POINTER(ctypes.c_int64)]),

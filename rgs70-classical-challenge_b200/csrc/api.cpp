@@ -118,6 +118,55 @@ int rgs_plan_step(const rgs_plan* plan, int32_t j, int32_t* v, int32_t* is_free,
   return RGS_OK;
 }
 
+int rgs_plan_set_fusion(rgs_plan* plan, int32_t on) {
+  if (!plan) return fail(RGS_ERR_ARG, "plan is NULL");
+  if (!plan->plan.device_copies.empty())
+    return fail(RGS_ERR_ARG, "fusion must be set before the plan's first use on a device");
+  plan_set_fusion(plan->plan, on != 0);
+  return RGS_OK;
+}
+
+int rgs_plan_pairs(const rgs_plan* plan, int32_t* count, int32_t* first_positions) {
+  if (!plan || !count) return fail(RGS_ERR_ARG, "null argument");
+  *count = (int32_t)plan->plan.pairs.size();
+  if (first_positions)
+    for (size_t k = 0; k < plan->plan.pairs.size(); ++k) first_positions[k] = plan->plan.pairs[k].j;
+  return RGS_OK;
+}
+
+int rgs_plan_pair_info(const rgs_plan* plan, int32_t k, rgs_pair_info* info) {
+  if (!plan || !info) return fail(RGS_ERR_ARG, "null argument");
+  if (k < 0 || k >= (int32_t)plan->plan.pairs.size()) return fail(RGS_ERR_ARG, "pair index out of range");
+  const DevPair& d = plan->plan.pairs[k];
+  *info = rgs_pair_info{};
+  info->j = d.j;
+  info->code_a = d.codeA;
+  info->code_b = d.codeB;
+  info->a = d.a;
+  info->m = d.m;
+  info->o = d.o;
+  info->dw = d.dw;
+  for (int i = 0; i < 3; ++i) info->piv[i] = d.piv[i];
+  info->pw_b = d.pwB;
+  info->mask_a = d.maskA;
+  info->beta_a = d.betaA;
+  for (int i = 0; i < 4; ++i) {
+    info->comb_a[i] = d.combA[i];
+    info->la_w[i] = d.LAw[i];
+  }
+  info->beta_b = d.betaB;
+  info->mb0[0] = d.MB0[0];
+  info->mb0[1] = d.MB0[1];
+  info->t_b = d.tB;
+  const PlanStep& A = plan->plan.steps[d.j];
+  const PlanStep& B = plan->plan.steps[d.j + 1];
+  for (int i = 0; i < d.m && i < 64; ++i) {
+    info->la_cols[i] = (uint64_t)A.lcols[i];
+    info->mb_cols[i] = (uint64_t)B.mcols[i];
+  }
+  return RGS_OK;
+}
+
 int rgs_plan_step_tables(const rgs_plan* plan, int32_t j, uint64_t* tables, int32_t* nbytes) {
   if (!plan) return fail(RGS_ERR_ARG, "plan is NULL");
   if (j < 0 || j >= plan->plan.n) return fail(RGS_ERR_ARG, "step index out of range");

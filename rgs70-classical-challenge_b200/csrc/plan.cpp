@@ -3,6 +3,7 @@
 #include "plan.hpp"
 
 #include <algorithm>
+#include <cmath>
 #include <map>
 
 namespace rgs {
@@ -120,6 +121,7 @@ void run_compiler(int n, const std::vector<u128>& later, const std::vector<int>&
         st.kernel.push_back(vec);
       }
       st.ycol = is_free ? columns[r_in] : 0;
+      st.mcols = columns;
     }
     basis.swap(rows);
   }
@@ -162,7 +164,196 @@ std::string rank_profile(int n, const std::vector<std::pair<int, int>>& edges, c
   return "";
 }
 
+void small_runs(const Plan& p, int& h, int& t) {
+  auto small = [&](int j) { return std::max(p.steps[j].r_in, p.steps[j].r_out) <= kSmallRank; };
+  h = 0;
+  while (h < p.n && small(h)) ++h;
+  t = p.n;
+  while (t > h && small(t - 1)) --t;
+}
+
 namespace {
+
+u128 apply_cols(const std::vector<u128>& cols, u128 x) {
+  u128 r = 0;
+  for (size_t i = 0; i < cols.size(); ++i)
+    if (bit_of(x, (int)i)) r ^= cols[i];
+  return r;
+}
+
+// Pair code of a step as it runs in a fused pair, or -1 if the pair kernel does not
+// cover it.  `basis` receives the listing basis of the step's projected combos (kappa-0
+// vectors first), used when the step is B.
+int pair_code(const PlanStep& st, const DevStep& d, std::vector<u128>& basis) {
+  basis.clear();
+  if (!st.free) return -1;
+  const u128 mask = one_at(st.r_in) - 1;
+  if (d.mode == MODE_MERGE) {
+    if (d.ncombos != 2) return -1;
+    basis.push_back((u128)d.combos[1] & mask);
+    return PC_M2;
+  }
+  if (d.mode != MODE_PAIR) return -1;
+  if (d.ncombos == 1) return PC_P1;
+  if (d.ncombos == 2) {
+    basis.push_back(st.kernel[0] & mask);
+    return bit_of(st.kernel[0], st.r_in) ? PC_P2H : PC_P2F;
+  }
+  // Four combos: one kappa-0 and one kappa-1 basis vector (kappa nonzero), else unsupported.
+  const u128 k1 = st.kernel[0], k2 = st.kernel[1];
+  const u128 cand[3] = {k1, k2, k1 ^ k2};
+  u128 zero = 0, one = 0;
+  bool has0 = false, has1 = false;
+  for (u128 c : cand) {
+    if (!bit_of(c, st.r_in) && !has0) {
+      zero = c;
+      has0 = true;
+    } else if (bit_of(c, st.r_in) && !has1) {
+      one = c;
+      has1 = true;
+    }
+  }
+  if (!has0 || !has1) return -1;
+  basis.push_back(zero & mask);
+  basis.push_back(one & mask);
+  return PC_P4H;
+}
+
+// Echelon pivots (highest bits, ascending) of the span of `vecs`; false if dependent.
+bool pivots_of(std::vector<u128> vecs, std::vector<int>& piv) {
+  piv.clear();
+  for (size_t i = 0; i < vecs.size(); ++i) {
+    u128 v = vecs[i];
+    for (size_t k = 0; k < i; ++k)
+      if (bit_of(v, highest_bit(vecs[k]))) v ^= vecs[k];
+    if (!v) return false;
+    vecs[i] = v;
+    // keep earlier vectors free of the new pivot so later reductions stay consistent
+    for (size_t k = 0; k < i; ++k)
+      if (bit_of(vecs[k], highest_bit(v))) vecs[k] ^= v;
+    piv.push_back(highest_bit(v));
+  }
+  std::sort(piv.begin(), piv.end());
+  return true;
+}
+
+// The pair record of positions j, j + 1, or false when they cannot be fused.
+bool make_pair(Plan& p, int j, DevPair& out, std::vector<unsigned long long>& mb_tables) {
+  const PlanStep& A = p.steps[j];
+  const PlanStep& B = p.steps[j + 1];
+  const DevStep& dA = p.dev[j];
+  const DevStep& dB = p.dev[j + 1];
+  std::vector<u128> basisA, basisB;
+  const int cA = pair_code(A, dA, basisA);
+  const int cB = pair_code(B, dB, basisB);
+  if (cA < 0 || cB < 0) return false;
+  const int m = A.r_out;
+  if (B.r_in != m || m < 1) return false;
+  const bool pairA = cA != PC_M2;
+  const u128 tA = pairA ? A.ycol : 0;
+  // t_A must lie outside span(basisB) (else W is smaller than the kernel assumes).
+  std::vector<u128> listing;
+  if (pairA) listing.push_back(tA);
+  for (u128 b : basisB) listing.push_back(b);
+  std::vector<int> piv;
+  if (!pivots_of(listing, piv)) return false;
+  const int dw = (int)listing.size();
+  if (dw > 3 || dw > m) return false;
+  const int nw = 1 << dw;
+  auto w_of = [&](int i) {
+    u128 w = 0;
+    for (int k = 0; k < dw; ++k)
+      if ((i >> k) & 1) w ^= listing[k];
+    return w;
+  };
+  DevPair d{};
+  d.j = j;
+  d.codeA = cA;
+  d.codeB = cB;
+  d.a = A.r_in;
+  d.m = m;
+  d.o = B.r_out;
+  d.maskA = (unsigned long long)(one_at(A.r_in) - 1);
+  d.betaA = (unsigned long long)A.beta;
+  for (int k = 0; k < 4; ++k) d.combA[k] = dA.combos[k];
+  d.betaB = (unsigned long long)B.beta;
+  d.tB = (unsigned long long)(cB == PC_M2 ? 0 : B.ycol);
+  const int ncb = 1 << (int)basisB.size();
+  const int na = ncb;  // A-units: pairs of registers (PAIR A) or single registers (MERGE A)
+  for (int u = 0; u < na; ++u) {
+    const u128 w = pairA ? w_of(2 * u) : w_of(u);
+    d.LAw[u] = (unsigned long long)apply_cols(A.lcols, w);
+  }
+  const std::vector<u128> mB(B.mcols.begin(), B.mcols.begin() + m);
+  d.MB0[0] = 0;
+  d.MB0[1] = pairA ? (unsigned long long)apply_cols(mB, tA) : 0;
+  d.pwB = 0;
+  for (int i = 0; i < nw; ++i) {
+    const u128 x = w_of(i) & B.beta;
+    const int par = (__builtin_popcountll((uint64_t)x) + __builtin_popcountll((uint64_t)(x >> 64))) & 1;
+    d.pwB |= (unsigned)par << i;
+  }
+  d.dw = dw;
+  for (int k = 0; k < 3; ++k) d.piv[k] = k < dw ? piv[k] : 0;
+  d.tabA_off = dA.table_off;
+  d.nbA = dA.nbytes;
+  std::vector<u128> tab;
+  int nb = 0;
+  byte_tables(mB, m, tab, nb);
+  d.tabMB_off = p.tables.size() + mb_tables.size();
+  d.nbMB = nb;
+  for (auto x : tab) mb_tables.push_back((unsigned long long)x);
+  out = d;
+  return true;
+}
+
+// Chooses the fused pairs: non-overlapping (j, j + 1) with j >= 1, inside one of the
+// leading / middle / trailing runs, maximising the intermediate entries kept out of
+// HBM (2^m each); rebuilds p.pairs and p.pair_at.
+void build_pairs(Plan& p) {
+  p.pairs.clear();
+  p.pair_at.assign(p.n, -1);
+  // Drop the byte tables of an earlier pair build (they follow the step tables).
+  size_t step_tables = 0;
+  for (auto& d : p.dev) step_tables = std::max(step_tables, (size_t)d.table_off + ((size_t)d.nbytes << 8));
+  p.tables.resize(step_tables);
+  if (!p.fuse || !p.exec_ok) return;
+  for (auto& st : p.steps)
+    if (!st.free) return;
+  int h = 0, t = 0;
+  small_runs(p, h, t);
+  auto region = [&](int j) { return j < h ? 0 : (j < t ? 1 : 2); };
+  std::vector<DevPair> cand(p.n);
+  std::vector<char> ok(p.n, 0);
+  std::vector<unsigned long long> scratch;
+  for (int j = 1; j + 1 < p.n; ++j) {
+    if (region(j) != region(j + 1)) continue;
+    scratch.clear();
+    ok[j] = make_pair(p, j, cand[j], scratch) ? 1 : 0;
+  }
+  std::vector<double> best(p.n + 2, 0.0);
+  std::vector<char> take(p.n + 1, 0);
+  for (int j = p.n - 1; j >= 0; --j) {
+    best[j] = best[j + 1];
+    if (ok[j]) {
+      const double g = std::ldexp(1.0, p.steps[j].r_out) + best[j + 2];
+      if (g > best[j]) {
+        best[j] = g;
+        take[j] = 1;
+      }
+    }
+  }
+  std::vector<unsigned long long> mb;
+  for (int j = 0; j < p.n; ++j) {
+    if (!take[j]) continue;
+    DevPair d;
+    make_pair(p, j, d, mb);
+    p.pair_at[j] = (int)p.pairs.size();
+    p.pairs.push_back(d);
+    ++j;
+  }
+  p.tables.insert(p.tables.end(), mb.begin(), mb.end());
+}
 
 // Builds the device records; fails (without error) when a step is too wide to execute.
 void build_device(Plan& p) {
@@ -219,9 +410,15 @@ void build_device(Plan& p) {
     for (int k = 0; k < 4; ++k) d.combos[k] = k < d.ncombos ? (unsigned long long)combos[k] : 0ull;
     p.dev.push_back(d);
   }
+  build_pairs(p);
 }
 
 }  // namespace
+
+void plan_set_fusion(Plan& p, bool on) {
+  p.fuse = on;
+  build_pairs(p);
+}
 
 std::string compile_plan(int n, const std::vector<std::pair<int, int>>& edges, const std::vector<int>& order,
                          const std::vector<uint8_t>& fixed, Plan& out) {

@@ -38,6 +38,7 @@ struct PlanStep {
   std::vector<u128> lcols;     // right inverse, r_out columns of r_in+free bits
   std::vector<u128> kernel;    // null space of (c, y) -> c', at most two vectors
   u128 ycol = 0;               // image of the y unit vector in new coordinates (free steps)
+  std::vector<u128> mcols;     // the map (c, y) -> c' itself: image of input bit i (i < r_in + free)
 };
 
 // Execution modes of one step on the device (derived, not part of the reference plan).
@@ -57,6 +58,45 @@ struct DevStep {
   int ng0;                       // MODE_PAIR: the first ng0 combos have y bit 0 (the rest y bit 1)
 };
 
+// Two consecutive free positions A = j and B = j + 1 run as one pass (scan_pair_kernel):
+// the intermediate table (A's output, B's input) stays in registers.  Rows of that
+// table fall into groups, cosets q0 + W of a subspace W (dim <= 3) closed under A's
+// output pairing and B's gathers; a group's inputs, its |W| intermediate rows and its
+// outputs involve no row of another group.  Intermediate row i of a group is
+// q0 ^ w_i, w_i = sum of listing-basis vectors by the bits of i: for PAIR A bit 0 is
+// A's pair offset t_A and the higher bits (B-term index) span B's projected combos
+// (kappa-0 vectors first); for MERGE A the bits span B's projected combos alone.
+enum PairCode : int {
+  PC_P1 = 0,   // PAIR, one combo
+  PC_P2H = 1,  // PAIR, two combos, the second with y bit 1
+  PC_P2F = 2,  // PAIR, two combos, both with y bit 0
+  PC_P4H = 3,  // PAIR, four combos, the last two with y bit 1
+  PC_M2 = 4,   // MERGE, two combos
+};
+constexpr int kPairCodes = 5;
+struct DevPair {
+  unsigned long long maskA, betaA;
+  unsigned long long combA[4];   // A's combos (step order: kappa-0 first)
+  unsigned long long LAw[4];     // L_A w of A-unit u's first row (with A's y bit)
+  unsigned long long betaB;
+  unsigned long long MB0[2];     // M_B (w | 0) of B-unit b's first row
+  unsigned long long tB;         // B's output pair offset (PAIR B)
+  unsigned long long tabA_off;   // A's byte tables (q -> L_A q over m bits)
+  unsigned long long tabMB_off;  // byte tables of q -> M_B (q | 0) over m bits
+  unsigned pwB;                  // bit i: parity(w_i & beta_B)
+  int a;                         // r_in(A): A's y bit
+  int m, o;                      // intermediate and output ranks
+  int nbA, nbMB;                 // byte counts of the two tables
+  int dw;                        // dim W: 2^(m - dw) groups
+  int piv[3];                    // pivot bits of W (ascending): a group's q0 has zeros there
+  int codeA, codeB;              // PairCode of A and B
+  int j;                         // position A
+};
+
+// Positions whose input and output ranks are both at most kSmallRank run once per chunk
+// of tiles (scan.cu); a fused pair never straddles the leading / middle / trailing split.
+constexpr int kSmallRank = 12;
+
 struct Plan {
   int n = 0;
   std::vector<int> order;
@@ -68,6 +108,10 @@ struct Plan {
   // Derived execution data (valid when executable()).
   std::vector<DevStep> dev;
   std::vector<unsigned long long> tables;  // concatenated byte tables
+  // Fused pairs: pair_at[j] >= 0 when positions j and j + 1 run as pairs[pair_at[j]].
+  std::vector<DevPair> pairs;
+  std::vector<int> pair_at;
+  bool fuse = true;                        // build fused pairs (plan_set_fusion)
   bool exec_ok = false;
   std::string exec_reason;
   // Device copies, per device ordinal (created lazily by the executor).
@@ -111,6 +155,14 @@ std::string order_search(int n, const std::vector<std::pair<int, int>>& edges, c
 void byte_tables(const std::vector<u128>& cols, int nbits, std::vector<u128>& out, int& nbytes);
 
 std::vector<u128> kernel_combos(const std::vector<u128>& kernel);
+
+// Leading / trailing runs of low-rank positions (input and output rank <= kSmallRank):
+// positions [0, h) and [t, n) (h <= t).
+void small_runs(const Plan& p, int& h, int& t);
+
+// Turns pair fusion on or off (rebuilds the pair records; the device copies are
+// refreshed by the executor).
+void plan_set_fusion(Plan& p, bool on);
 
 }  // namespace rgs
 

@@ -256,11 +256,8 @@ int scan_chunk_layout(const Plan& plan, int Bt, int precision, int S, ChunkLayou
   if (rc) return rc;
   if (S < 1) return fail(RGS_ERR_ARG, "chunk must hold at least one tile");
   const int n = plan.n;
-  auto small = [&](int j) { return std::max(plan.steps[j].r_in, plan.steps[j].r_out) <= kSmallRank; };
-  int h = 0;
-  while (h < n && small(h)) ++h;
-  int t = n;
-  while (t > h && small(t - 1)) --t;
+  int h = 0, t = 0;
+  small_runs(plan, h, t);
   int rs = 0, rmid = 0;
   for (int j = 0; j < n; ++j) {
     const int r = std::max(plan.steps[j].r_in, plan.steps[j].r_out);
@@ -374,6 +371,67 @@ cudaError_t launch_step(int precision, int Bt, int device, cudaStream_t s, const
 #undef RGS_MODES
 }
 
+int pair_nc(int code) { return code == PC_P1 ? 1 : (code == PC_P4H ? 4 : 2); }
+
+// Fused pair (j, j + 1) over `tiles` tiles: grid of 256-thread blocks whose warp count is
+// a multiple of the row's column slices (a warp keeps one slice).
+cudaError_t launch_pair(int precision, int Bt, int device, cudaStream_t s, const void* Ein, void* Eout,
+                        const DevPair& P, const u64* tables, const double4* WA, const double4* WB, const u64* mp,
+                        u64* mA, u64* mc, int tiles = 1, u64 es = 0) {
+  const int lbt = __builtin_ctz((unsigned)Bt);
+  const int VE = (precision != RGS_PREC_C128 && Bt >= 2) ? 2 : 1;
+  const int lC = lbt - (VE == 2 ? 1 : 0);
+  const int lL = lC < 5 ? lC : 5;
+  const int lS = lC - lL;
+  if (lS > 3) return cudaErrorInvalidValue;  // more column slices than warps in a block
+  const int loads = pair_nc(P.codeA) * pair_nc(P.codeB);
+  const int U = loads >= 8 ? 1 : 8 / loads;
+  const unsigned long long groups = 1ull << (P.m - P.dw);
+  const unsigned long long per_warp = (unsigned long long)U << (5 - lL);
+  const unsigned long long warps = ((groups + per_warp - 1) / per_warp) << lS;
+  const long long cap = (long long)sm_count(device) * 16;
+  const long long blocks = std::max<long long>(1, std::min<long long>((long long)((warps + 7) / 8), cap));
+  const dim3 grid((unsigned)blocks, (unsigned)tiles);
+  if (precision == RGS_PREC_C128) return launch_pair_c128(VE, grid, s, Ein, Eout, P, tables, WA, WB, mp, mA, mc, lbt, es);
+  if (precision == RGS_PREC_C64) return launch_pair_c64(VE, grid, s, Ein, Eout, P, tables, WA, WB, mp, mA, mc, lbt, es);
+  return launch_pair_f32(VE, grid, s, Ein, Eout, P, tables, WA, WB, mp, mA, mc, lbt, es);
+}
+
+// The sweep as segments: one position, or a fused pair (plan.pair_at).
+struct Segment {
+  int j, len, pair;
+};
+std::vector<Segment> segments_of(const Plan& plan, int from, int to) {
+  std::vector<Segment> out;
+  for (int j = from; j < to;) {
+    const int pa = plan.pair_at.empty() ? -1 : plan.pair_at[j];
+    if (pa >= 0 && j + 1 < to) {
+      out.push_back({j, 2, pa});
+      j += 2;
+    } else {
+      out.push_back({j, 1, -1});
+      j += 1;
+    }
+  }
+  return out;
+}
+
+// One segment over `tiles` tiles: rows of weights / maxima start at W / mx (item stride
+// `stride` between positions).
+cudaError_t launch_segment(const Plan& plan, const Segment& g, int precision, int Bt, int device, cudaStream_t s,
+                           const void* Ein, void* Eout, const u64* tables, const double4* W,
+                           const unsigned char* F, u64* mx, size_t stride, int tiles, u64 es) {
+  const int j = g.j;
+  if (g.len == 2)
+    return launch_pair(precision, Bt, device, s, Ein, Eout, plan.pairs[g.pair], tables, W + (size_t)j * stride,
+                       W + (size_t)(j + 1) * stride, mx + (size_t)(j - 1) * stride, mx + (size_t)j * stride,
+                       mx + (size_t)(j + 1) * stride, tiles, es);
+  const DevStep& st = plan.dev[j];
+  return launch_step(precision, Bt, device, s, Ein, Eout, st, tables + st.table_off, W + (size_t)j * stride,
+                     F ? F + (size_t)j * stride : nullptr, j ? mx + (size_t)(j - 1) * stride : nullptr,
+                     mx + (size_t)j * stride, j == 0, tiles, es);
+}
+
 bool plan_has_fixed(const Plan& p) {
   for (auto& st : p.steps)
     if (!st.free) return true;
@@ -406,14 +464,17 @@ int scan_launch_count(const Plan& plan, long long batch, int Bt, int precision, 
   const long long n = plan.n;
   long long total = 0;
   if (S < 2) {
-    total = (batch + Bt - 1) / Bt * (n + 2);
+    total = (batch + Bt - 1) / Bt * ((long long)segments_of(plan, 0, (int)n).size() + 2);
   } else {
     const long long stride = (long long)S * Bt;
+    const long long nh = (long long)segments_of(plan, 0, C.h).size();
+    const long long nm = (long long)segments_of(plan, C.h, C.t).size();
+    const long long nt = (long long)segments_of(plan, std::max(C.t, C.h), (int)n).size();
     for (long long first = 0; first < batch; first += stride) {
       const long long tiles = (std::min(stride, batch - first) + Bt - 1) / Bt;
-      total += 1 + C.h;
-      if (C.h < C.t) total += tiles * (C.t - C.h) + (C.t == n ? tiles : 0);
-      if (C.t < n || C.h == n) total += n - std::max(C.t, C.h) + 1;
+      total += 1 + nh;
+      if (C.h < C.t) total += tiles * nm + (C.t == n ? tiles : 0);
+      if (C.t < n || C.h == n) total += nt + 1;
     }
   }
   *out = total;
@@ -450,6 +511,7 @@ int scan_run_tiles(Plan& plan, const double* U, const u64* bits, const double* f
   u64* maxbuf = (u64*)(ws + L.off_max);
   const u64* tables = (const u64*)dc->tables;
   long long launches = 0;
+  const std::vector<Segment> segs = segments_of(plan, 0, plan.n);
 
   for (long long first = 0; first < batch; first += Bt) {
     const int count = (int)std::min<long long>(Bt, batch - first);
@@ -458,14 +520,14 @@ int scan_run_tiles(Plan& plan, const double* U, const u64* bits, const double* f
     RGS_CUDA_TRY(cudaGetLastError());
     RGS_CUDA_TRY(cudaMemsetAsync(maxbuf, 0, (size_t)plan.n * Bt * sizeof(u64), stream));
     launches += 1;
-    for (int j = 0; j < plan.n; ++j) {
-      const DevStep& st = plan.dev[j];
-      RGS_CUDA_TRY(launch_step(precision, Bt, device, stream, buf[j & 1], buf[(j + 1) & 1], st, tables + st.table_off,
-                               W + (size_t)j * Bt, F ? F + (size_t)j * Bt : nullptr,
-                               j ? maxbuf + (size_t)(j - 1) * Bt : nullptr, maxbuf + (size_t)j * Bt, j == 0));
+    int cur = 0;
+    for (const Segment& g : segs) {
+      RGS_CUDA_TRY(launch_segment(plan, g, precision, Bt, device, stream, buf[cur], buf[cur ^ 1], tables, W, F,
+                                  maxbuf, (size_t)Bt, 1, 0));
+      cur ^= 1;
       launches += 1;
     }
-    const void* fin = buf[plan.n & 1];
+    const void* fin = buf[cur];
     if (precision == RGS_PREC_C128)
       scan_finalize_kernel<double><<<(count + 127) / 128, 128, 0, stream>>>(
           (const double*)fin, maxbuf, plan.n, Bt, count, (double*)out_value + 2 * first, out_logscale + first);
@@ -515,9 +577,8 @@ int scan_run(Plan& plan, const double* U, const u64* bits, const double* fvec, l
   const u64* tables = (const u64*)dc->tables;
   const int lbt = __builtin_ctz((unsigned)Bt);
   long long launches = 0;
-  auto wrow = [&](int j) { return W + (size_t)j * stride; };
-  auto frow = [&](int j) { return F ? F + (size_t)j * stride : nullptr; };
-  auto mrow = [&](int j) { return maxbuf + (size_t)j * stride; };
+  const std::vector<Segment> head = segments_of(plan, 0, h), mid = segments_of(plan, h, t),
+                             tail = segments_of(plan, std::max(t, h), n);
 
   for (long long first = 0; first < batch; first += stride) {
     const int count = (int)std::min<long long>(stride, batch - first);
@@ -530,38 +591,39 @@ int scan_run(Plan& plan, const double* U, const u64* bits, const double* fvec, l
     launches += 1;
     int cur = 0;
     // Leading small positions: all tiles of the chunk per launch.
-    for (int j = 0; j < h; ++j) {
-      const DevStep& st = plan.dev[j];
-      RGS_CUDA_TRY(launch_step(precision, Bt, device, stream, small[cur], small[cur ^ 1], st, tables + st.table_off,
-                               wrow(j), frow(j), j ? mrow(j - 1) : nullptr, mrow(j), j == 0, tiles, C.e_stride));
+    for (const Segment& g : head) {
+      RGS_CUDA_TRY(launch_segment(plan, g, precision, Bt, device, stream, small[cur], small[cur ^ 1], tables, W, F,
+                                  maxbuf, (size_t)stride, tiles, C.e_stride));
       cur ^= 1;
       launches += 1;
     }
     // Middle positions, tile by tile: from the tile's slice of the small buffer through the
     // full-size tables to its slice of the other small buffer (or to the final value).
-    if (h < t) {
+    if (!mid.empty()) {
       for (int k = 0; k < tiles; ++k) {
         const size_t koff = (size_t)k * C.e_stride * esize;
-        for (int j = h; j < t; ++j) {
-          const DevStep& st = plan.dev[j];
-          const void* in = j == h ? (const void*)(small[cur] + koff) : (const void*)big[(j - h) & 1];
-          void* out = (j == t - 1 && t < n) ? (void*)(small[cur ^ 1] + koff) : (void*)big[(j - h + 1) & 1];
-          RGS_CUDA_TRY(launch_step(precision, Bt, device, stream, in, out, st, tables + st.table_off,
-                                   wrow(j) + (size_t)k * Bt, frow(j) ? frow(j) + (size_t)k * Bt : nullptr,
-                                   j ? mrow(j - 1) + (size_t)k * Bt : nullptr, mrow(j) + (size_t)k * Bt, j == 0));
+        const size_t ik = (size_t)k * Bt;
+        int bb = 0;
+        for (size_t gi = 0; gi < mid.size(); ++gi) {
+          const bool first_seg = gi == 0, last_seg = gi + 1 == mid.size();
+          const void* in = first_seg ? (const void*)(small[cur] + koff) : (const void*)big[bb];
+          void* out = (last_seg && t < n) ? (void*)(small[cur ^ 1] + koff) : (void*)big[first_seg ? 0 : bb ^ 1];
+          RGS_CUDA_TRY(launch_segment(plan, mid[gi], precision, Bt, device, stream, in, out, tables, W + ik,
+                                      F ? F + ik : nullptr, maxbuf + ik, (size_t)stride, 1, 0));
+          if (!first_seg) bb ^= 1;
           launches += 1;
         }
         if (t == n) {  // the sweep ends in the full-size tables: finalise this tile now
           const int kc = std::min(Bt, count - k * Bt);
-          const void* fin = big[(t - h) & 1];
+          const void* fin = big[mid.size() == 1 ? 0 : bb];
           if (precision == RGS_PREC_C128)
             scan_finalize_chunk_kernel<double><<<(kc + 127) / 128, 128, 0, stream>>>(
-                (const double*)fin, 0ull, lbt, maxbuf + (size_t)k * Bt, n, stride, kc,
-                (double*)out_value + 2 * (first + (long long)k * Bt), out_logscale + first + (long long)k * Bt);
+                (const double*)fin, 0ull, lbt, maxbuf + ik, n, stride, kc,
+                (double*)out_value + 2 * (first + (long long)ik), out_logscale + first + (long long)ik);
           else
             scan_finalize_chunk_kernel<float><<<(kc + 127) / 128, 128, 0, stream>>>(
-                (const float*)fin, 0ull, lbt, maxbuf + (size_t)k * Bt, n, stride, kc,
-                (float*)out_value + 2 * (first + (long long)k * Bt), out_logscale + first + (long long)k * Bt);
+                (const float*)fin, 0ull, lbt, maxbuf + ik, n, stride, kc,
+                (float*)out_value + 2 * (first + (long long)ik), out_logscale + first + (long long)ik);
           RGS_CUDA_TRY(cudaGetLastError());
           launches += 1;
         }
@@ -570,10 +632,9 @@ int scan_run(Plan& plan, const double* U, const u64* bits, const double* fvec, l
     }
     // Trailing small positions: all tiles per launch again.
     if (t < n || h == n) {
-      for (int j = std::max(t, h); j < n; ++j) {
-        const DevStep& st = plan.dev[j];
-        RGS_CUDA_TRY(launch_step(precision, Bt, device, stream, small[cur], small[cur ^ 1], st, tables + st.table_off,
-                                 wrow(j), frow(j), j ? mrow(j - 1) : nullptr, mrow(j), j == 0, tiles, C.e_stride));
+      for (const Segment& g : tail) {
+        RGS_CUDA_TRY(launch_segment(plan, g, precision, Bt, device, stream, small[cur], small[cur ^ 1], tables, W,
+                                    F, maxbuf, (size_t)stride, tiles, C.e_stride));
         cur ^= 1;
         launches += 1;
       }

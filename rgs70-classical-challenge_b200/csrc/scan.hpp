@@ -28,7 +28,6 @@ int scan_layout(const Plan& plan, int Bt, int precision, ScanLayout& L);
 // rank at most kSmallRank); the positions between the leading and trailing small ones
 // (h <= j < t) run tile by tile.  Workspace: two small-table buffers of S tiles, two
 // full-size tables for the middle positions, weights / flags / maxima of S tiles.
-constexpr int kSmallRank = 12;
 constexpr int kChunkItems = 8192;  // default items per chunk (S = kChunkItems / Bt tiles)
 struct ChunkLayout {
   int Bt = 1, S = 1, h = 0, t = 0;
@@ -44,6 +43,20 @@ int scan_chunk_tiles(int Bt);
 int scan_pick_chunk(const Plan& plan, int Bt, int precision, size_t ws_bytes, ChunkLayout& C, int* S);
 // Kernel launches scan_run queues for `batch` items with that workspace.
 int scan_launch_count(const Plan& plan, long long batch, int Bt, int precision, size_t ws_bytes, long long* out);
+
+// Fused pair launches (scan_pair_{c128,c64,f32}.cu): one instantiation set per precision.
+cudaError_t launch_pair_c128(int VE, dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevPair& P,
+                             const unsigned long long* tables, const double4* WA, const double4* WB,
+                             const unsigned long long* mp, unsigned long long* mA, unsigned long long* mc, int lbt,
+                             unsigned long long es);
+cudaError_t launch_pair_c64(int VE, dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevPair& P,
+                            const unsigned long long* tables, const double4* WA, const double4* WB,
+                            const unsigned long long* mp, unsigned long long* mA, unsigned long long* mc, int lbt,
+                            unsigned long long es);
+cudaError_t launch_pair_f32(int VE, dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevPair& P,
+                            const unsigned long long* tables, const double4* WA, const double4* WB,
+                            const unsigned long long* mp, unsigned long long* mA, unsigned long long* mc, int lbt,
+                            unsigned long long es);
 
 // Largest batch tile the step kernel supports for a precision.
 int scan_max_tile(int precision);

@@ -31,6 +31,14 @@ __device__ __forceinline__ void cmad(Cx<M>& acc, M er, M ei, const Cx<M>& w) {
   acc.im = fma(ei, w.re, acc.im);
 }
 
+// x with its sign flipped iff neg (exact).
+__device__ __forceinline__ float flip_sign(float x, int neg) {
+  return __int_as_float(__float_as_int(x) ^ (neg << 31));
+}
+__device__ __forceinline__ double flip_sign(double x, int neg) {
+  return __hiloint2double(__double2hiint(x) ^ (neg << 31), __double2loint(x));
+}
+
 // |x|^2 with a fixed rounding sequence.
 template <typename S>
 __device__ __forceinline__ S norm2(S re, S im) {

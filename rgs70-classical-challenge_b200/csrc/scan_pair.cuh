@@ -1,0 +1,236 @@
+// Fused pair kernel: scan positions A = j and B = j + 1 in one pass over HBM.
+//
+// The unfused sweep writes A's output table and reads it back for B.  Here a warp (or a
+// sub-warp, for rows shorter than 32 chunks) takes one group of rows at a time (DevPair,
+// plan.hpp): the group's input rows of A are gathered once, A's outputs for the group
+// (the |W| intermediate rows, at most 8) are formed in registers and rounded to the
+// storage type exactly as the unfused step stores them, and B's outputs of the group are
+// formed from those registers and stored.  Every intermediate row belongs to exactly
+// one group, so each input entry is read once and each output entry written once; the
+// intermediate table never reaches memory.
+//
+// Renormalisation.  A is scaled by 2^-e from the previous maximum as usual; B runs
+// unscaled (the scale of an intermediate table is not known until the whole table
+// exists) and the pass records max |E|^2 = 1/4 for A, whose exponent is 0, so the
+// finalisation's sum of exponents stays exact; B's maximum is recorded as usual and
+// scales the position after B.  A value therefore differs from the unfused sweep's by an
+// exact power of two in (value, logscale), not in the amplitude value * 2^logscale.
+//
+// Lanes: a lane owns one 16-byte chunk column of every row it touches (VE items);
+// rows of more than 32 chunks are split into 32-chunk column slices, one slice per
+// warp (the grid's warp count is a multiple of the slice count).
+#pragma once
+#include "scan_device.cuh"
+
+namespace rgs {
+
+template <int C>
+struct PairMode {
+  static constexpr bool pair = C != PC_M2;
+  static constexpr int nc = C == PC_P1 ? 1 : (C == PC_P4H ? 4 : 2);
+  static constexpr int ng0 = C == PC_P1 ? 1 : (C == PC_P2H ? 1 : (C == PC_P2F ? 2 : (C == PC_P4H ? 2 : 2)));
+};
+
+__device__ __forceinline__ u64 deposit_pivots(u64 it, const DevPair& P) {
+  u64 q = it;
+  for (int k = 0; k < P.dw; ++k) q = deposit_zero(q, P.piv[k]);
+  return q;
+}
+
+template <typename S, typename M, int VE, int CA, int CB>
+__global__ void __launch_bounds__(256, 1)
+    scan_pair_kernel(const S* __restrict__ Ein, S* __restrict__ Eout, const __grid_constant__ DevPair P,
+                     const u64* __restrict__ tables, const double4* __restrict__ WA, const double4* __restrict__ WB,
+                     const u64* __restrict__ maxprev, u64* __restrict__ maxA, u64* __restrict__ maxcur, int lbt,
+                     u64 e_stride) {
+  using MA = PairMode<CA>;
+  using MB = PairMode<CB>;
+  constexpr int NCA = MA::nc, NCB = MB::nc;
+  constexpr int NW = MA::pair ? 2 * NCB : NCB;  // intermediate rows per group
+  constexpr int NUA = NCB;                      // A units: register pairs (PAIR A) or registers
+  constexpr int NUB = MA::pair ? 2 : 1;         // B units
+  constexpr int LOADS = NUA * NCA;
+  constexpr int U = LOADS >= 8 ? 1 : 8 / LOADS;  // groups per lane per iteration
+  __shared__ u64 smax[256];
+  const int Bt = 1 << lbt;
+  const int lC = lbt - (VE == 2 ? 1 : 0);  // log2 chunks per row
+  const int lL = lC < 5 ? lC : 5;          // log2 lanes per row
+  const int lR = 5 - lL;                   // log2 groups side by side in a warp
+  const int lS = lC - lL;                  // log2 column slices per row
+  const int lane = threadIdx.x & 31;
+  const int sub = lane >> lL;
+  const int l = lane & ((1 << lL) - 1);
+
+  if (blockIdx.y) {  // tile k of a chunk of tiles
+    const u64 k = blockIdx.y;
+    Ein += 2 * k * e_stride;
+    Eout += 2 * k * e_stride;
+    WA += k << lbt;
+    WB += k << lbt;
+    maxprev += k << lbt;
+    maxA += k << lbt;
+    maxcur += k << lbt;
+  }
+  for (int i = threadIdx.x; i < Bt; i += blockDim.x) smax[i] = 0;
+  if (blockIdx.x == 0)
+    for (int i = threadIdx.x; i < Bt; i += blockDim.x) maxA[i] = max_bits<S>((S)0.25);
+
+  const u64 gwarp = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  const u64 slice = gwarp & ((1ull << lS) - 1ull);
+  const u64 col = (slice << 5) + (u64)l;  // this lane's chunk column
+
+  Cx<M> wAa[VE], wAb[VE], wBa[VE], wBb[VE];
+#pragma unroll
+  for (int v = 0; v < VE; ++v) {
+    const int b = (int)(col * VE) + v;
+    const double s = ldexp(1.0, -scale_exponent(max_value<S>(maxprev[b])));
+    const double4 fa = WA[b], fb = WB[b];
+    double ar = fa.x * s, ai = fa.y * s, br = fa.z * s, bi = fa.w * s;
+    if (!MA::pair) {
+      const double pr = ar + br, pi = ai + bi, mr = ar - br, mi = ai - bi;
+      ar = pr, ai = pi, br = mr, bi = mi;
+    }
+    wAa[v] = Cx<M>{(M)ar, (M)ai};
+    wAb[v] = Cx<M>{(M)br, (M)bi};
+    double cr = fb.x, ci = fb.y, dr = fb.z, di = fb.w;
+    if (!MB::pair) {
+      const double pr = cr + dr, pi = ci + di, mr = cr - dr, mi = ci - di;
+      cr = pr, ci = pi, dr = mr, di = mi;
+    }
+    wBa[v] = Cx<M>{(M)cr, (M)ci};
+    wBb[v] = Cx<M>{(M)dr, (M)di};
+  }
+  __syncthreads();
+
+  const u64* TA = tables + P.tabA_off;
+  const u64* TMB = tables + P.tabMB_off;
+  const u64 groups = 1ull << (P.m - P.dw);
+  const u64 per_iter = (u64)U << lR;
+  const u64 wslice = nwarps >> lS;  // warps per column slice
+  S mx[VE];
+#pragma unroll
+  for (int v = 0; v < VE; ++v) mx[v] = (S)0;
+
+  for (u64 base = (gwarp >> lS) * per_iter; base < groups; base += wslice * per_iter) {
+    bool ok[U];
+    u64 c0[U];
+    int pq[U], ya[U][NUA], pa[U][NUA][NCA];
+    Chunk<S, VE> e[U][NUA][NCA];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const u64 it = base + ((u64)u << lR) + sub;
+      ok[u] = it < groups;
+      const u64 q0 = ok[u] ? deposit_pivots(it, P) : 0ull;
+      const u64 p0 = ok[u] ? table_lookup(TA, P.nbA, q0) : 0ull;
+      c0[u] = ok[u] ? table_lookup(TMB, P.nbMB, q0) : 0ull;
+      pq[u] = __popcll(q0 & P.betaB) & 1;
+#pragma unroll
+      for (int a = 0; a < NUA; ++a) {
+        const u64 pu = p0 ^ P.LAw[a];
+        ya[u][a] = (int)((pu >> P.a) & 1ull);
+#pragma unroll
+        for (int k = 0; k < NCA; ++k) {
+          const u64 row = (pu ^ P.combA[k]) & P.maskA;
+          pa[u][a][k] = __popcll(row & P.betaA) & 1;
+          if (ok[u]) e[u][a][k].load(Ein, (row << lC) + col);
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (!ok[u]) continue;
+      Chunk<S, VE> outX[NUB], outY[NUB];
+#pragma unroll
+      for (int v = 0; v < VE; ++v) {
+        S ir[NW], ii[NW];
+        // A: the group's intermediate rows, rounded to the storage type.
+#pragma unroll
+        for (int a = 0; a < NUA; ++a) {
+          if (MA::pair) {
+            Cx<M> x{(M)0, (M)0}, y{(M)0, (M)0};
+#pragma unroll
+            for (int k = 0; k < NCA; ++k) {
+              const M er = (M)e[u][a][k].re(v), ei = (M)e[u][a][k].im(v);
+              const M nr = flip_sign(er, pa[u][a][k]), ni = flip_sign(ei, pa[u][a][k]);
+              if (k < MA::ng0) {
+                cmad(x, er, ei, wAa[v]);
+                cmad(y, nr, ni, wAb[v]);
+              } else {
+                cmad(x, nr, ni, wAb[v]);
+                cmad(y, er, ei, wAa[v]);
+              }
+            }
+            const S xr = (S)x.re, xi = (S)x.im, yr = (S)y.re, yi = (S)y.im;
+            const bool sw = ya[u][a];
+            ir[2 * a] = sw ? yr : xr;
+            ii[2 * a] = sw ? yi : xi;
+            ir[2 * a + 1] = sw ? xr : yr;
+            ii[2 * a + 1] = sw ? xi : yi;
+          } else {
+            Cx<M> x{(M)0, (M)0};
+#pragma unroll
+            for (int k = 0; k < NCA; ++k)
+              cmad(x, (M)e[u][a][k].re(v), (M)e[u][a][k].im(v), pa[u][a][k] ? wAb[v] : wAa[v]);
+            ir[a] = (S)x.re;
+            ii[a] = (S)x.im;
+          }
+        }
+        // B: the group's output rows from the registers.
+#pragma unroll
+        for (int b = 0; b < NUB; ++b) {
+          Cx<M> x{(M)0, (M)0}, y{(M)0, (M)0};
+#pragma unroll
+          for (int a = 0; a < NCB; ++a) {
+            const int i = MA::pair ? (a << 1) | b : a;
+            const int par = pq[u] ^ (int)((P.pwB >> i) & 1u);
+            const M er = (M)ir[i], ei = (M)ii[i];
+            if (MB::pair) {
+              const M nr = flip_sign(er, par), ni = flip_sign(ei, par);
+              if (a < MB::ng0) {
+                cmad(x, er, ei, wBa[v]);
+                cmad(y, nr, ni, wBb[v]);
+              } else {
+                cmad(x, nr, ni, wBb[v]);
+                cmad(y, er, ei, wBa[v]);
+              }
+            } else {
+              cmad(x, er, ei, par ? wBb[v] : wBa[v]);
+            }
+          }
+          const S xr = (S)x.re, xi = (S)x.im;
+          outX[b].set(v, xr, xi);
+          mx[v] = fmax(mx[v], norm2(xr, xi));
+          if (MB::pair) {
+            const S yr = (S)y.re, yi = (S)y.im;
+            outY[b].set(v, yr, yi);
+            mx[v] = fmax(mx[v], norm2(yr, yi));
+          }
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < NUB; ++b) {
+        const u64 cx = c0[u] ^ P.MB0[b];
+        outX[b].store(Eout, (cx << lC) + col);
+        if (MB::pair) outY[b].store(Eout, ((cx ^ P.tB) << lC) + col);
+      }
+    }
+  }
+
+  // Maximum |E|^2 of B's outputs per item: lanes of other groups in the warp that own
+  // the same column, then shared memory, then one global atomicMax per item per block.
+#pragma unroll
+  for (int v = 0; v < VE; ++v) {
+    u64 bits = max_bits<S>(mx[v]);
+    for (int off = 16; off >= (1 << lL); off >>= 1) {
+      const u64 o = __shfl_xor_sync(0xffffffffu, bits, off);
+      bits = bits > o ? bits : o;
+    }
+    if (sub == 0 && bits) atomicMax(&smax[(int)(col * VE) + v], bits);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < Bt; i += blockDim.x)
+    if (smax[i]) atomicMax(&maxcur[i], smax[i]);
+}
+
+}  // namespace rgs

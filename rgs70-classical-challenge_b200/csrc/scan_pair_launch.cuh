@@ -1,0 +1,47 @@
+// Launch dispatch of scan_pair_kernel over the 25 (A, B) pair codes, instantiated per
+// storage / arithmetic type in scan_pair_{c128,c64,f32}.cu.
+#pragma once
+#include "scan_pair.cuh"
+
+namespace rgs {
+
+template <typename S, typename M, int VE, int CA, int CB>
+cudaError_t launch_pair_one(dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevPair& P,
+                            const u64* tables, const double4* WA, const double4* WB, const u64* mp, u64* mA,
+                            u64* mc, int lbt, u64 es) {
+  scan_pair_kernel<S, M, VE, CA, CB><<<grid, 256, 0, s>>>((const S*)Ein, (S*)Eout, P, tables, WA, WB, mp, mA, mc,
+                                                           lbt, es);
+  return cudaGetLastError();
+}
+
+template <typename S, typename M, int VE, int CA>
+cudaError_t launch_pair_b(dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevPair& P,
+                          const u64* tables, const double4* WA, const double4* WB, const u64* mp, u64* mA, u64* mc,
+                          int lbt, u64 es) {
+#define RGS_PAIR_B(CB) launch_pair_one<S, M, VE, CA, CB>(grid, s, Ein, Eout, P, tables, WA, WB, mp, mA, mc, lbt, es)
+  switch (P.codeB) {
+    case PC_P1: return RGS_PAIR_B(PC_P1);
+    case PC_P2H: return RGS_PAIR_B(PC_P2H);
+    case PC_P2F: return RGS_PAIR_B(PC_P2F);
+    case PC_P4H: return RGS_PAIR_B(PC_P4H);
+    default: return RGS_PAIR_B(PC_M2);
+  }
+#undef RGS_PAIR_B
+}
+
+template <typename S, typename M, int VE>
+cudaError_t launch_pair_codes(dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevPair& P,
+                              const u64* tables, const double4* WA, const double4* WB, const u64* mp, u64* mA,
+                              u64* mc, int lbt, u64 es) {
+#define RGS_PAIR_A(CA) launch_pair_b<S, M, VE, CA>(grid, s, Ein, Eout, P, tables, WA, WB, mp, mA, mc, lbt, es)
+  switch (P.codeA) {
+    case PC_P1: return RGS_PAIR_A(PC_P1);
+    case PC_P2H: return RGS_PAIR_A(PC_P2H);
+    case PC_P2F: return RGS_PAIR_A(PC_P2F);
+    case PC_P4H: return RGS_PAIR_A(PC_P4H);
+    default: return RGS_PAIR_A(PC_M2);
+  }
+#undef RGS_PAIR_A
+}
+
+}  // namespace rgs

@@ -48,14 +48,6 @@ struct ChunkGroup {
   static constexpr int value = CPL < cap ? CPL : cap;
 };
 
-// x with its sign flipped iff neg (exact).
-__device__ __forceinline__ float flip_sign(float x, int neg) {
-  return __int_as_float(__float_as_int(x) ^ (neg << 31));
-}
-__device__ __forceinline__ double flip_sign(double x, int neg) {
-  return __hiloint2double(__double2hiint(x) ^ (neg << 31), __double2loint(x));
-}
-
 template <typename S, typename M, int VE, int MODE, int NC, int CPL, int NG0>
 __global__ void __launch_bounds__(256, 2) scan_row_kernel(const S* __restrict__ Ein, S* __restrict__ Eout,
                                                        const __grid_constant__ DevStep st,

@@ -54,7 +54,7 @@ def _u128(lo, hi):
 class ScanPlan:
     """A compiled scan order (opaque native handle plus exported views)."""
 
-    def __init__(self, n, edges, order, fixed=frozenset()):
+    def __init__(self, n, edges, order, fixed=frozenset(), fuse=True):
         L = _lib.lib()
         self.n = int(n)
         self.edges = [tuple(map(int, x)) for x in edges]
@@ -65,6 +65,8 @@ class ScanPlan:
         _lib.check(L.rgs_plan_compile(self.n, len(e), _lib.ptr(e, ctypes.c_int32), _lib.ptr(o, ctypes.c_int32),
                                       None if f is None else _lib.ptr(f, ctypes.c_uint8), ctypes.byref(handle)))
         self._h = handle
+        if not fuse:
+            _lib.check(L.rgs_plan_set_fusion(self._h, 0))
         n32, rmax, ex = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
         _lib.check(L.rgs_plan_info(self._h, ctypes.byref(n32), ctypes.byref(rmax), ctypes.byref(ex)))
         self.rmax = int(rmax.value)
@@ -77,6 +79,22 @@ class ScanPlan:
     @property
     def handle(self):
         return self._h
+
+    @property
+    def pairs(self):
+        """Positions j whose pair (j, j + 1) runs fused (one pass, no intermediate table)."""
+        L = _lib.lib()
+        cnt = ctypes.c_int32()
+        _lib.check(L.rgs_plan_pairs(self._h, ctypes.byref(cnt), None))
+        out = np.zeros(max(1, cnt.value), dtype=np.int32)
+        _lib.check(L.rgs_plan_pairs(self._h, ctypes.byref(cnt), _lib.ptr(out, ctypes.c_int32)))
+        return out[:cnt.value].tolist()
+
+    def pair_info(self, k):
+        """The k-th fused pair's record (``rgs_pair_info``)."""
+        info = _lib.PairInfo()
+        _lib.check(_lib.lib().rgs_plan_pair_info(self._h, int(k), ctypes.byref(info)))
+        return info
 
     @property
     def sum_states(self):

@@ -256,10 +256,11 @@ class ScanOracle:
     ``source`` is accepted for signature compatibility and ignored (the engine is
     this package).  ``fp64`` selects complex128 tables (the reference's FP64
     rescoring kernel); otherwise complex64 tables with float64 weights and sums.
+    ``fuse=False`` runs every position as its own pass (no fused pairs).
     """
 
     def __init__(self, g, u, order, source=None, device=0, gpu=True, fp64=False, precision=None,
-                 batch_tile=None, memory_budget=None):
+                 batch_tile=None, memory_budget=None, fuse=True):
         if not gpu:
             raise ValueError("this engine has no CPU executor; the CPU restatement is the test oracle")
         g = np.asarray(g)
@@ -267,7 +268,7 @@ class ScanOracle:
         self.u = np.asarray(u)
         self.order = list(order)
         self.edges = edges_from_graph(g)
-        self.plan = ScanPlan(self.n, self.edges, self.order)
+        self.plan = ScanPlan(self.n, self.edges, self.order, fuse=fuse)
         self.ranks = self.plan.ranks
         self.rmax = self.plan.rmax
         self.gpu = True

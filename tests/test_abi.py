@@ -54,10 +54,20 @@ def _launches(pkg, plan, batch, tile, prec, ws):
     return out.value
 
 
+def _segments(plan, lo, hi):
+    """Launches of positions [lo, hi): one per position, one per fused pair."""
+    pairs = set(plan.pairs)
+    count, j = 0, lo
+    while j < hi:
+        j += 2 if (j in pairs and j + 1 < hi) else 1
+        count += 1
+    return count
+
+
 def test_scan_launch_schedule(pkg):
     """Launch count of a sweep: with the full workspace, the low-rank leading and trailing
-    positions run once per chunk of tiles; with a one-tile workspace, every position runs
-    once per tile (n steps + weights + finalisation)."""
+    positions run once per chunk of tiles; with a one-tile workspace, every segment (a
+    position or a fused pair) runs once per tile, plus weights and finalisation."""
     inst = pkg.instances.make_instance("reg3", 40, 40, pkg.rank_profile)
     plan = pkg.ScanPlan(inst.n, pkg.edges_from_graph(inst.g), inst.order)
     n, ranks = inst.n, list(plan.ranks)
@@ -78,13 +88,14 @@ def test_scan_launch_schedule(pkg):
             expect = 0
             for first in range(0, batch, chunk):
                 tiles = -(-min(chunk, batch - first) // tile)
-                expect += 1 + h
+                expect += 1 + _segments(plan, 0, h)
                 if h < t:
-                    expect += tiles * (t - h) + (tiles if t == n else 0)
+                    expect += tiles * _segments(plan, h, t) + (tiles if t == n else 0)
                 if t < n or h == n:
-                    expect += n - max(t, h) + 1
+                    expect += _segments(plan, max(t, h), n) + 1
             assert _launches(pkg, plan, batch, tile, prec, ws.value) == expect, (tile, batch)
         # One tile's tables only: the tile-by-tile schedule.
         per_tile = 2 * ((tile << max(ranks)) * 8) + n * tile * (32 + 1 + 8)
         got = _launches(pkg, plan, 1000, tile, prec, per_tile + 4096)
-        assert got == -(-1000 // tile) * (n + 2)
+        assert got == -(-1000 // tile) * (_segments(plan, 0, n) + 2)
+    assert plan.pairs

@@ -1,8 +1,9 @@
 """Resident batch executor (many small instances, one persistent launch) against the
 streaming executor, the chain-rule sampler and the FP64 statevector oracle.
 
-* Amplitudes are bitwise equal to the streaming executor's (same weights, fma order and
-  renormalisation), for every precision, uneven instance sizes and fixed vertices.
+* Amplitudes are bitwise equal to the streaming executor's run position by position
+  (``fuse=False``: same weights, fma order and renormalisation), for every precision,
+  uneven instance sizes and fixed vertices.
 * Samples equal the streaming chain sampler's for the same seed (the two sum branch
   masses in different orders, so a decision whose uniform lies within rounding of a
   branch boundary may differ: at most 1%), and follow the Born distribution.
@@ -45,7 +46,7 @@ def test_amplitudes_bitwise_equal_streaming(pkg, precision):
     rb.run()
     for k, inst in enumerate(insts):
         val, ls, amp = rb.amplitudes(k)
-        eng = pkg.ScanEngine(pkg.ScanPlan(inst.n, pkg.edges_from_graph(inst.g), inst.order), inst.u,
+        eng = pkg.ScanEngine(pkg.ScanPlan(inst.n, pkg.edges_from_graph(inst.g), inst.order, fuse=False), inst.u,
                              precision=precision)
         rv, rls = eng.sweep_bits(bits[k])
         assert np.array_equal(val, rv) and np.array_equal(ls, rls), (k, inst.name)
@@ -81,7 +82,7 @@ def test_uneven_batch_and_largest_rank(pkg):
     rb.run()
     for k, inst in enumerate(insts):
         val, ls, _ = rb.amplitudes(k)
-        so = pkg.ScanOracle(inst.g, inst.u, inst.order)
+        so = pkg.ScanOracle(inst.g, inst.u, inst.order, fuse=False)
         rv, rls = so.engine.sweep_bits(bits[k])
         assert np.array_equal(val, rv) and np.array_equal(ls, rls), inst.name
 
@@ -217,7 +218,7 @@ def test_tuned_launch_variants(pkg):
         rb.run()
         for k, inst in enumerate(insts):
             val, ls, _ = rb.amplitudes(k)
-            rv, rls = pkg.ScanOracle(inst.g, inst.u, inst.order).engine.sweep_bits(bits[k])
+            rv, rls = pkg.ScanOracle(inst.g, inst.u, inst.order, fuse=False).engine.sweep_bits(bits[k])
             assert np.array_equal(val, rv) and np.array_equal(ls, rls)
             sb, p, lp = rb.samples(k)
             assert np.abs(lp - np.log(p)).max() < 1e-4

@@ -1,0 +1,205 @@
+"""Fused pairs of scan positions (host side, no GPU).
+
+The compiler's pair records (``rgs_plan_pair_info``) are executed here by a NumPy
+emulation of the pair kernel's group walk (groups q0 + W, A units, B units) and compared
+with the two positions run one after the other by the oracle's step rule
+(``scan_plan.py:161-195``): same outputs, every input row read once, every output row
+written once.  Also: which pairs are chosen, and that fusion can be switched off.
+"""
+import numpy as np
+import pytest
+
+from oracle import scan_plan as sp
+
+PAIR_NC = {0: 1, 1: 2, 2: 2, 3: 4, 4: 2}
+PAIR_NG0 = {0: 1, 1: 1, 2: 2, 3: 2, 4: 2}
+
+
+def _parity(x):
+    return bin(int(x)).count("1") & 1
+
+
+def _apply(cols, x):
+    r = 0
+    for i, c in enumerate(cols):
+        if (x >> i) & 1:
+            r ^= int(c)
+    return r
+
+
+def _oracle_step(env, st, f0, f1):
+    """One free position of the oracle sweep, without renormalisation."""
+    tables = sp.byte_tables(st.Lcols, st.r_out)
+    out = np.zeros(1 << st.r_out, dtype=np.complex128)
+    mask = (1 << st.r_in) - 1
+    combos = sp.kernel_combos(st.kernel)
+    for c in range(1 << st.r_out):
+        p0 = 0
+        for b in range(tables.shape[0]):
+            p0 ^= int(tables[b][(c >> (8 * b)) & 255])
+        acc = 0j
+        for combo in combos:
+            p = p0 ^ int(combo)
+            row = p & mask
+            y = (p >> st.r_in) & 1
+            sign = -1.0 if (y and _parity(row & st.beta)) else 1.0
+            acc += env[row] * sign * (f1 if y else f0)
+        out[c] = acc
+    return out
+
+
+def _deposit(it, piv):
+    q = it
+    for p in piv:
+        low = (1 << p) - 1
+        q = ((q & ~low) << 1) | (q & low)
+    return q
+
+
+def _emulate_pair(info, env, fa, fb):
+    """The pair kernel's computation for one item, in complex128."""
+    ca, cb = info.code_a, info.code_b
+    pair_a, pair_b = ca != 4, cb != 4
+    nca, ncb = PAIR_NC[ca], PAIR_NC[cb]
+    ng0a, ng0b = PAIR_NG0[ca], PAIR_NG0[cb]
+    nua, nub = ncb, (2 if pair_a else 1)
+    nw = 2 * ncb if pair_a else ncb
+    m, dw = info.m, info.dw
+    piv = [info.piv[k] for k in range(dw)]
+    la = [info.la_cols[i] for i in range(m)]
+    mb = [info.mb_cols[i] for i in range(m)]
+    if pair_a:
+        wa, wb = fa
+    else:
+        wa, wb = fa[0] + fa[1], fa[0] - fa[1]
+    if pair_b:
+        va, vb = fb
+    else:
+        va, vb = fb[0] + fb[1], fb[0] - fb[1]
+    out = np.zeros(1 << info.o, dtype=np.complex128)
+    written = np.zeros(1 << info.o, dtype=np.int64)
+    read = np.zeros(len(env), dtype=np.int64)
+    for it in range(1 << (m - dw)):
+        q0 = _deposit(it, piv)
+        p0 = _apply(la, q0)
+        c0 = _apply(mb, q0)
+        pq = _parity(q0 & info.beta_b)
+        reg = [0j] * nw
+        for a in range(nua):
+            pu = p0 ^ int(info.la_w[a])
+            ya = (pu >> info.a) & 1
+            terms = []
+            for k in range(nca):
+                row = (pu ^ int(info.comb_a[k])) & int(info.mask_a)
+                read[row] += 1
+                terms.append((env[row], _parity(row & info.beta_a)))
+            if pair_a:
+                x = y = 0j
+                for k, (e, par) in enumerate(terms):
+                    n = -e if par else e
+                    if k < ng0a:
+                        x += e * wa
+                        y += n * wb
+                    else:
+                        x += n * wb
+                        y += e * wa
+                reg[2 * a], reg[2 * a + 1] = (y, x) if ya else (x, y)
+            else:
+                reg[a] = sum(e * (wb if par else wa) for e, par in terms)
+        for b in range(nub):
+            x = y = 0j
+            for a in range(ncb):
+                i = (a << 1) | b if pair_a else a
+                par = pq ^ ((info.pw_b >> i) & 1)
+                e = reg[i]
+                n = -e if par else e
+                if pair_b:
+                    if a < ng0b:
+                        x += e * va
+                        y += n * vb
+                    else:
+                        x += n * vb
+                        y += e * va
+                else:
+                    x += e * (vb if par else va)
+            cx = c0 ^ int(info.mb0[b])
+            out[cx] = x
+            written[cx] += 1
+            if pair_b:
+                out[cx ^ int(info.t_b)] = y
+                written[cx ^ int(info.t_b)] += 1
+    return out, written, read
+
+
+def _instances(pkg):
+    rng = np.random.default_rng(12)
+    out = []
+    for kind, n in (("reg3", 14), ("reg3", 18), ("er3", 16), ("deg3", 20), ("dense", 12), ("dense", 14)):
+        for s in range(3):
+            if kind == "dense":
+                g = pkg.instances.dense(n, rng)
+                order = rng.permutation(n).tolist()
+                out.append((g, order))
+            else:
+                inst = pkg.instances.make_instance(kind, n, int(rng.integers(1 << 30)), pkg.rank_profile)
+                out.append((inst.g, inst.order))
+                out.append((inst.g, rng.permutation(n).tolist()))
+    return out
+
+
+def test_pair_records_match_two_oracle_steps(pkg):
+    rng = np.random.default_rng(5)
+    codes = set()
+    npairs = 0
+    for g, order in _instances(pkg):
+        n = g.shape[0]
+        edges = pkg.edges_from_graph(g)
+        plan = pkg.ScanPlan(n, edges, order)
+        steps, _ = sp.make_plan(n, [tuple(e) for e in edges], order)
+        for k, j in enumerate(plan.pairs):
+            info = plan.pair_info(k)
+            assert info.j == j and 1 <= j < n - 1
+            A, B = steps[j], steps[j + 1]
+            if A.r_out > 12 or A.r_in > 12 or B.r_out > 12:
+                continue
+            env = rng.normal(size=1 << A.r_in) + 1j * rng.normal(size=1 << A.r_in)
+            fa = rng.normal(size=2) + 1j * rng.normal(size=2)
+            fb = rng.normal(size=2) + 1j * rng.normal(size=2)
+            ref = _oracle_step(_oracle_step(env, A, *fa), B, *fb)
+            got, written, read = _emulate_pair(info, env, fa, fb)
+            assert np.all(written == 1), (j, info.code_a, info.code_b)
+            assert np.all(read == 1), (j, info.code_a, info.code_b)
+            assert np.allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max()), (j, info.code_a, info.code_b)
+            codes.add((info.code_a, info.code_b))
+            npairs += 1
+    assert npairs >= 40
+    # Rising, peak and falling pairs of 3-regular plans, and the merge codes.
+    assert {(0, 0), (0, 3), (3, 3), (3, 4), (4, 4)} <= codes, codes
+
+
+def test_pairs_chosen_and_switch(pkg):
+    inst = pkg.instances.make_instance("reg3", 24, 3, pkg.rank_profile)
+    edges = pkg.edges_from_graph(inst.g)
+    plan = pkg.ScanPlan(inst.n, edges, inst.order)
+    pairs = plan.pairs
+    assert pairs and all(b - a >= 2 for a, b in zip(pairs, pairs[1:]))
+    assert 0 not in pairs and all(j + 1 < inst.n for j in pairs)
+    # The pairs skip the largest intermediate tables: the peak rank is never materialised
+    # when a pair around it is allowed.
+    off = pkg.ScanPlan(inst.n, edges, inst.order, fuse=False)
+    assert off.pairs == []
+    # Plans with fixed vertices are not fused.
+    fx = pkg.ScanPlan(inst.n, edges, inst.order, frozenset({inst.order[3]}))
+    assert fx.pairs == []
+
+
+def test_fusion_switch_after_use_is_rejected(pkg):
+    import ctypes
+    inst = pkg.instances.make_instance("reg3", 10, 3, pkg.rank_profile)
+    plan = pkg.ScanPlan(inst.n, pkg.edges_from_graph(inst.g), inst.order)
+    # Before any device use the switch is accepted (host only).
+    pkg._lib.check(pkg._lib.lib().rgs_plan_set_fusion(plan.handle, 0))
+    pkg._lib.check(pkg._lib.lib().rgs_plan_set_fusion(plan.handle, 1))
+    cnt = ctypes.c_int32()
+    pkg._lib.check(pkg._lib.lib().rgs_plan_pairs(plan.handle, ctypes.byref(cnt), None))
+    assert cnt.value == len(plan.pairs)
