@@ -37,8 +37,15 @@ __device__ __forceinline__ u64 deposit_pivots(u64 it, const DevPair& P) {
   return q;
 }
 
+// Two 256-thread blocks per SM (128 registers) where the registers suffice; one for
+// float64 arithmetic on complex64 tables, whose conversions need more.
+template <typename S, typename M>
+struct PairBlocks {
+  static constexpr int value = sizeof(M) > sizeof(S) ? 1 : 2;
+};
+
 template <typename S, typename M, int VE, int CA, int CB>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(256, PairBlocks<S, M>::value)
     scan_pair_kernel(const S* __restrict__ Ein, S* __restrict__ Eout, const __grid_constant__ DevPair P,
                      const u64* __restrict__ tables, const double4* __restrict__ WA, const double4* __restrict__ WB,
                      const u64* __restrict__ maxprev, u64* __restrict__ maxA, u64* __restrict__ maxcur, int lbt,
