@@ -31,9 +31,35 @@ struct PairMode {
   static constexpr int ng0 = C == PC_P1 ? 1 : (C == PC_P2H ? 1 : (C == PC_P2F ? 2 : (C == PC_P4H ? 2 : 2)));
 };
 
-__device__ __forceinline__ u64 deposit_pivots(u64 it, const DevPair& P) {
-  u64 q = it;
-  for (int k = 0; k < P.dw; ++k) q = deposit_zero(q, P.piv[k]);
+// Group index arithmetic in the index type I: 32-bit where every rank of the pair is at
+// most 31 (fewer instructions per group), 64-bit otherwise.
+template <typename I>
+__device__ __forceinline__ int parity_of(I x);
+template <>
+__device__ __forceinline__ int parity_of<unsigned>(unsigned x) {
+  return __popc(x) & 1;
+}
+template <>
+__device__ __forceinline__ int parity_of<u64>(u64 x) {
+  return __popcll(x) & 1;
+}
+
+// Byte-table map of c (the XOR of one table entry per byte of c).
+template <typename I>
+__device__ __forceinline__ I lookup_as(const u64* __restrict__ T, int nbytes, I c) {
+  I p = 0;
+  for (int b = 0; b < nbytes; ++b) p ^= (I)__ldg(T + (b << 8) + (int)((c >> (8 * b)) & (I)255));
+  return p;
+}
+
+// Group representative q0: the group index with zeros inserted at W's pivots.
+template <typename I>
+__device__ __forceinline__ I deposit_pivots(I it, const DevPair& P) {
+  I q = it;
+  for (int k = 0; k < P.dw; ++k) {
+    const I low = ((I)1 << P.piv[k]) - (I)1;
+    q = ((q & ~low) << 1) | (q & low);
+  }
   return q;
 }
 
@@ -44,7 +70,7 @@ struct PairBlocks {
   static constexpr int value = sizeof(M) > sizeof(S) ? 1 : 2;
 };
 
-template <typename S, typename M, int VE, int CA, int CB>
+template <typename S, typename M, int VE, int CA, int CB, typename I>
 __global__ void __launch_bounds__(256, PairBlocks<S, M>::value)
     scan_pair_kernel(const S* __restrict__ Ein, S* __restrict__ Eout, const __grid_constant__ DevPair P,
                      const u64* __restrict__ tables, const double4* __restrict__ WA, const double4* __restrict__ WB,
@@ -112,6 +138,7 @@ __global__ void __launch_bounds__(256, PairBlocks<S, M>::value)
 
   const u64* TA = tables + P.tabA_off;
   const u64* TMB = tables + P.tabMB_off;
+  const I maskA = (I)P.maskA, betaA = (I)P.betaA, betaB = (I)P.betaB;
   const u64 groups = 1ull << (P.m - P.dw);
   const u64 per_iter = (u64)U << lR;
   const u64 wslice = nwarps >> lS;  // warps per column slice
@@ -121,26 +148,26 @@ __global__ void __launch_bounds__(256, PairBlocks<S, M>::value)
 
   for (u64 base = (gwarp >> lS) * per_iter; base < groups; base += wslice * per_iter) {
     bool ok[U];
-    u64 c0[U];
+    I c0[U];
     int pq[U], ya[U][NUA], pa[U][NUA][NCA];
     Chunk<S, VE> e[U][NUA][NCA];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const u64 it = base + ((u64)u << lR) + sub;
       ok[u] = it < groups;
-      const u64 q0 = ok[u] ? deposit_pivots(it, P) : 0ull;
-      const u64 p0 = ok[u] ? table_lookup(TA, P.nbA, q0) : 0ull;
-      c0[u] = ok[u] ? table_lookup(TMB, P.nbMB, q0) : 0ull;
-      pq[u] = __popcll(q0 & P.betaB) & 1;
+      const I q0 = ok[u] ? deposit_pivots<I>((I)it, P) : (I)0;
+      const I p0 = ok[u] ? lookup_as<I>(TA, P.nbA, q0) : (I)0;
+      c0[u] = ok[u] ? lookup_as<I>(TMB, P.nbMB, q0) : (I)0;
+      pq[u] = parity_of<I>(q0 & betaB);
 #pragma unroll
       for (int a = 0; a < NUA; ++a) {
-        const u64 pu = p0 ^ P.LAw[a];
-        ya[u][a] = (int)((pu >> P.a) & 1ull);
+        const I pu = p0 ^ (I)P.LAw[a];
+        ya[u][a] = (int)((pu >> P.a) & (I)1);
 #pragma unroll
         for (int k = 0; k < NCA; ++k) {
-          const u64 row = (pu ^ P.combA[k]) & P.maskA;
-          pa[u][a][k] = __popcll(row & P.betaA) & 1;
-          if (ok[u]) e[u][a][k].load(Ein, (row << lC) + col);
+          const I row = (pu ^ (I)P.combA[k]) & maskA;
+          pa[u][a][k] = parity_of<I>(row & betaA);
+          if (ok[u]) e[u][a][k].load(Ein, ((u64)row << lC) + col);
         }
       }
     }
@@ -217,9 +244,9 @@ __global__ void __launch_bounds__(256, PairBlocks<S, M>::value)
       }
 #pragma unroll
       for (int b = 0; b < NUB; ++b) {
-        const u64 cx = c0[u] ^ P.MB0[b];
-        outX[b].store(Eout, (cx << lC) + col);
-        if (MB::pair) outY[b].store(Eout, ((cx ^ P.tB) << lC) + col);
+        const I cx = c0[u] ^ (I)P.MB0[b];
+        outX[b].store(Eout, ((u64)cx << lC) + col);
+        if (MB::pair) outY[b].store(Eout, ((u64)(cx ^ (I)P.tB) << lC) + col);
       }
     }
   }

@@ -1,24 +1,24 @@
-// Launch dispatch of scan_pair_kernel over the 25 (A, B) pair codes, instantiated per
-// storage / arithmetic type in scan_pair_{c128,c64,f32}.cu.
+// Launch dispatch of scan_pair_kernel over the 25 (A, B) pair codes and the two index
+// widths, instantiated per storage / arithmetic type in scan_pair_{c128,c64,f32}.cu.
 #pragma once
 #include "scan_pair.cuh"
 
 namespace rgs {
 
-template <typename S, typename M, int VE, int CA, int CB>
+template <typename S, typename M, int VE, int CA, int CB, typename I>
 cudaError_t launch_pair_one(dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevPair& P,
                             const u64* tables, const double4* WA, const double4* WB, const u64* mp, u64* mA,
                             u64* mc, int lbt, u64 es) {
-  scan_pair_kernel<S, M, VE, CA, CB><<<grid, 256, 0, s>>>((const S*)Ein, (S*)Eout, P, tables, WA, WB, mp, mA, mc,
+  scan_pair_kernel<S, M, VE, CA, CB, I><<<grid, 256, 0, s>>>((const S*)Ein, (S*)Eout, P, tables, WA, WB, mp, mA, mc,
                                                            lbt, es);
   return cudaGetLastError();
 }
 
-template <typename S, typename M, int VE, int CA>
+template <typename S, typename M, int VE, int CA, typename I>
 cudaError_t launch_pair_b(dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevPair& P,
                           const u64* tables, const double4* WA, const double4* WB, const u64* mp, u64* mA, u64* mc,
                           int lbt, u64 es) {
-#define RGS_PAIR_B(CB) launch_pair_one<S, M, VE, CA, CB>(grid, s, Ein, Eout, P, tables, WA, WB, mp, mA, mc, lbt, es)
+#define RGS_PAIR_B(CB) launch_pair_one<S, M, VE, CA, CB, I>(grid, s, Ein, Eout, P, tables, WA, WB, mp, mA, mc, lbt, es)
   switch (P.codeB) {
     case PC_P1: return RGS_PAIR_B(PC_P1);
     case PC_P2H: return RGS_PAIR_B(PC_P2H);
@@ -29,11 +29,11 @@ cudaError_t launch_pair_b(dim3 grid, cudaStream_t s, const void* Ein, void* Eout
 #undef RGS_PAIR_B
 }
 
-template <typename S, typename M, int VE>
-cudaError_t launch_pair_codes(dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevPair& P,
-                              const u64* tables, const double4* WA, const double4* WB, const u64* mp, u64* mA,
-                              u64* mc, int lbt, u64 es) {
-#define RGS_PAIR_A(CA) launch_pair_b<S, M, VE, CA>(grid, s, Ein, Eout, P, tables, WA, WB, mp, mA, mc, lbt, es)
+template <typename S, typename M, int VE, typename I>
+cudaError_t launch_pair_a(dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevPair& P,
+                          const u64* tables, const double4* WA, const double4* WB, const u64* mp, u64* mA, u64* mc,
+                          int lbt, u64 es) {
+#define RGS_PAIR_A(CA) launch_pair_b<S, M, VE, CA, I>(grid, s, Ein, Eout, P, tables, WA, WB, mp, mA, mc, lbt, es)
   switch (P.codeA) {
     case PC_P1: return RGS_PAIR_A(PC_P1);
     case PC_P2H: return RGS_PAIR_A(PC_P2H);
@@ -42,6 +42,17 @@ cudaError_t launch_pair_codes(dim3 grid, cudaStream_t s, const void* Ein, void* 
     default: return RGS_PAIR_A(PC_M2);
   }
 #undef RGS_PAIR_A
+}
+
+// 32-bit group index arithmetic when the pair's input (with its y bit), intermediate and
+// output ranks all fit in 31 bits.
+template <typename S, typename M, int VE>
+cudaError_t launch_pair_codes(dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevPair& P,
+                              const u64* tables, const double4* WA, const double4* WB, const u64* mp, u64* mA,
+                              u64* mc, int lbt, u64 es) {
+  if (P.a <= 30 && P.m <= 31 && P.o <= 31)
+    return launch_pair_a<S, M, VE, unsigned>(grid, s, Ein, Eout, P, tables, WA, WB, mp, mA, mc, lbt, es);
+  return launch_pair_a<S, M, VE, u64>(grid, s, Ein, Eout, P, tables, WA, WB, mp, mA, mc, lbt, es);
 }
 
 }  // namespace rgs
