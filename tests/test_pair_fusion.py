@@ -254,3 +254,54 @@ def test_rgs70_pair_records_on_sampled_groups(pkg, fixtures):
             for row, val in outs:
                 ref = _oracle_at(B, row, lambda q: _oracle_at(A, q, env, *fa), *fb)
                 assert abs(val - ref) <= 1e-12 * max(1.0, abs(ref)), (j, row)
+
+
+RARE_CODES = {(2, 2), (3, 0), (4, 0), (4, 1)}
+
+
+def rare_code_plans(pkg):
+    """Small seeded plans that fuse the pair codes the larger test graphs do not produce
+    (a searched, deterministic list: one (graph, order) per code)."""
+    found = {}
+    rng = np.random.default_rng(9)
+    for t in range(3000):
+        n = int(rng.integers(8, 15))
+        kind = t % 4
+        if kind == 0:
+            g = pkg.instances.dense(n, rng)
+        else:
+            name = ["reg3", "er3", "deg3"][kind - 1]
+            if name == "reg3" and n % 2:
+                name = "er3"
+            g = pkg.instances.make_instance(name, n, int(rng.integers(1 << 30)), pkg.rank_profile).g
+        order = rng.permutation(n).tolist()
+        plan = pkg.ScanPlan(n, pkg.edges_from_graph(g), order)
+        for k in range(len(plan.pairs)):
+            info = plan.pair_info(k)
+            c = (info.code_a, info.code_b)
+            if c in RARE_CODES and c not in found:
+                found[c] = (g, order)
+        if len(found) == len(RARE_CODES):
+            break
+    return found
+
+
+def test_rare_pair_codes(pkg):
+    plans = rare_code_plans(pkg)
+    assert set(plans) == RARE_CODES
+    rng = np.random.default_rng(6)
+    for code, (g, order) in plans.items():
+        n = len(g)
+        edges = pkg.edges_from_graph(g)
+        plan = pkg.ScanPlan(n, edges, order)
+        steps, _ = sp.make_plan(n, [tuple(e) for e in edges], order)
+        for k, j in enumerate(plan.pairs):
+            info = plan.pair_info(k)
+            A, B = steps[j], steps[j + 1]
+            env = rng.normal(size=1 << A.r_in) + 1j * rng.normal(size=1 << A.r_in)
+            fa = rng.normal(size=2) + 1j * rng.normal(size=2)
+            fb = rng.normal(size=2) + 1j * rng.normal(size=2)
+            ref = _oracle_step(_oracle_step(env, A, *fa), B, *fb)
+            got, written, read = _emulate_pair(info, env, fa, fb)
+            assert np.all(written == 1) and np.all(read == 1), code
+            assert np.allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max()), code

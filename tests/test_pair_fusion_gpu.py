@@ -132,3 +132,23 @@ def test_launch_count_with_pairs(pkg):
     off = pkg.ScanEngine(pkg.ScanPlan(30, pkg.edges_from_graph(inst.g), inst.order, fuse=False), inst.u,
                          precision="c64f32", batch_tile=64)
     assert on.launch_count(64) == off.launch_count(64) - len(on.plan.pairs)
+
+
+def test_rare_pair_codes_on_gpu(pkg):
+    """The four pair codes the graphs above do not produce, on small seeded plans that do
+    (the same plans as the CPU emulation test), against the statevector."""
+    from test_pair_fusion import RARE_CODES, rare_code_plans
+    plans = rare_code_plans(pkg)
+    assert set(plans) == RARE_CODES
+    rng = np.random.default_rng(8)
+    for code, (g, order) in plans.items():
+        n = len(g)
+        u = pkg.instances.haar_su2(n, rng)
+        plan = pkg.ScanPlan(n, pkg.edges_from_graph(g), order)
+        bits = pkg.instances.uniform_bits(100, n, rng)
+        ref = np.abs(gs.statevector(g, u)[(bits.astype(np.int64) << np.arange(n)).sum(axis=1)]) ** 2
+        for precision in ("c64", "c64f32", "c128"):
+            for tile in (1, 8, pkg.max_batch_tile(precision)):
+                eng = pkg.ScanEngine(plan, u, precision=precision, batch_tile=tile)
+                p = _prob(pkg, *eng.sweep_bits(bits), n)
+                assert np.max(np.abs(p - ref) / ref) < TOL[precision], (code, precision, tile)
