@@ -300,9 +300,16 @@ bool make_pair(Plan& p, int j, DevPair& out, std::vector<unsigned long long>& mb
   std::vector<u128> tab;
   int nb = 0;
   byte_tables(mB, m, tab, nb);
-  d.tabMB_off = p.tables.size() + mb_tables.size();
+  if (nb != dA.nbytes) return false;
+  // One 16-byte entry per (byte, value): A's table entry and M_B's, so the kernel reads
+  // both maps of a group with one load per byte.
+  if ((p.tables.size() + mb_tables.size()) & 1) mb_tables.push_back(0ull);
+  d.tab2_off = p.tables.size() + mb_tables.size();
   d.nbMB = nb;
-  for (auto x : tab) mb_tables.push_back((unsigned long long)x);
+  for (size_t i = 0; i < tab.size(); ++i) {
+    mb_tables.push_back(p.tables[dA.table_off + i]);
+    mb_tables.push_back((unsigned long long)tab[i]);
+  }
   out = d;
   return true;
 }

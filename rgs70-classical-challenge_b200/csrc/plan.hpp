@@ -82,7 +82,8 @@ struct DevPair {
   unsigned long long MB0[2];     // M_B (w | 0) of B-unit b's first row
   unsigned long long tB;         // B's output pair offset (PAIR B)
   unsigned long long tabA_off;   // A's byte tables (q -> L_A q over m bits)
-  unsigned long long tabMB_off;  // byte tables of q -> M_B (q | 0) over m bits
+  unsigned long long tab2_off;   // interleaved tables over m bits: entry (b, v) is the pair
+                                 // (L_A part, M_B (. | 0) part), 16-byte aligned
   unsigned pwB;                  // bit i: parity(w_i & beta_B)
   int a;                         // r_in(A): A's y bit
   int m, o;                      // intermediate and output ranks

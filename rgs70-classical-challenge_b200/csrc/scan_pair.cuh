@@ -44,12 +44,17 @@ __device__ __forceinline__ int parity_of<u64>(u64 x) {
   return __popcll(x) & 1;
 }
 
-// Byte-table map of c (the XOR of one table entry per byte of c).
+// Both maps of a group from the interleaved byte tables (the XOR of one entry per byte
+// of c): p = L_A c, q = M_B (c | 0).
 template <typename I>
-__device__ __forceinline__ I lookup_as(const u64* __restrict__ T, int nbytes, I c) {
-  I p = 0;
-  for (int b = 0; b < nbytes; ++b) p ^= (I)__ldg(T + (b << 8) + (int)((c >> (8 * b)) & (I)255));
-  return p;
+__device__ __forceinline__ void lookup2_as(const u64* __restrict__ T2, int nbytes, I c, I& p, I& q) {
+  p = 0;
+  q = 0;
+  for (int b = 0; b < nbytes; ++b) {
+    const ulonglong2 t = __ldg(reinterpret_cast<const ulonglong2*>(T2) + (b << 8) + (int)((c >> (8 * b)) & (I)255));
+    p ^= (I)t.x;
+    q ^= (I)t.y;
+  }
 }
 
 // Group representative q0: the group index with zeros inserted at W's pivots.
@@ -136,8 +141,7 @@ __global__ void __launch_bounds__(256, PairBlocks<S, M>::value)
   }
   __syncthreads();
 
-  const u64* TA = tables + P.tabA_off;
-  const u64* TMB = tables + P.tabMB_off;
+  const u64* T2 = tables + P.tab2_off;
   const I maskA = (I)P.maskA, betaA = (I)P.betaA, betaB = (I)P.betaB;
   const u64 groups = 1ull << (P.m - P.dw);
   const u64 per_iter = (u64)U << lR;
@@ -156,8 +160,9 @@ __global__ void __launch_bounds__(256, PairBlocks<S, M>::value)
       const u64 it = base + ((u64)u << lR) + sub;
       ok[u] = it < groups;
       const I q0 = ok[u] ? deposit_pivots<I>((I)it, P) : (I)0;
-      const I p0 = ok[u] ? lookup_as<I>(TA, P.nbA, q0) : (I)0;
-      c0[u] = ok[u] ? lookup_as<I>(TMB, P.nbMB, q0) : (I)0;
+      I p0 = 0, cq = 0;
+      if (ok[u]) lookup2_as<I>(T2, P.nbMB, q0, p0, cq);
+      c0[u] = cq;
       pq[u] = parity_of<I>(q0 & betaB);
 #pragma unroll
       for (int a = 0; a < NUA; ++a) {
