@@ -209,6 +209,21 @@ def test_pairs_chosen_and_switch(pkg):
     # when a pair around it is allowed.
     off = pkg.ScanPlan(inst.n, edges, inst.order, fuse=False)
     assert off.pairs == []
+    # No pair straddles the low-rank head / middle / tail split of the chunked sweep
+    # (positions whose input and output ranks are at most 12 run once per chunk).
+    for g, order in _instances(pkg)[:12]:
+        plan = pkg.ScanPlan(len(g), pkg.edges_from_graph(g), order)
+        r = plan.ranks
+        small = [max(r[j - 1] if j else 0, r[j]) <= 12 for j in range(len(r))]
+        h = 0
+        while h < len(r) and small[h]:
+            h += 1
+        t = len(r)
+        while t > h and small[t - 1]:
+            t -= 1
+        region = [0 if j < h else (1 if j < t else 2) for j in range(len(r))]
+        for j in plan.pairs:
+            assert region[j] == region[j + 1]
     # Plans with fixed vertices are not fused.
     fx = pkg.ScanPlan(inst.n, edges, inst.order, frozenset({inst.order[3]}))
     assert fx.pairs == []
