@@ -41,6 +41,25 @@ def build_instance(pkg):
                                        order_seeds=ORDER_SEEDS)
 
 
+def _instances_module():
+    """The package's seeded instance generator (pure NumPy), loaded from its file alone so
+    that the reference arm never imports the package or loads librgs_b200.so."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("rgs_instances_only",
+                                                  ROOT / "rgs70-classical-challenge_b200" / "instances.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def build_instance_cpu():
+    """The bench instance with the scan order chosen by the oracle's rank profile (the
+    reference compiler restated), bit-identical to build_instance's."""
+    from oracle import scan_plan as sp
+    return _instances_module().make_instance("reg3", N_QUBITS, GRAPH_SEED, sp.rank_profile,
+                                             target_rank=TARGET_RANK, order_seeds=ORDER_SEEDS)
+
+
 def step_bytes(ranks, esize, pairs=()):
     """Compulsory table traffic of one sweep: every input entry read once, every output
     written once (step 0 reads the implicit unit table); a fused pair (j, j + 1) neither
@@ -156,12 +175,10 @@ def host_cores():
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    import __graft_entry__
-    pkg = __graft_entry__.package()
-    inst = build_instance(pkg)
+    inst = build_instance_cpu()
     cores = host_cores()
     rng = np.random.default_rng(BITS_SEED)
-    bits = pkg.instances.uniform_bits(BATCH, N_QUBITS, rng)
+    bits = _instances_module().uniform_bits(BATCH, N_QUBITS, rng)
     per_core = 2
     times = []
     for it in range(args.warmup + args.steps):
@@ -181,8 +198,109 @@ def run_reference(args, rank, world):
                          "sample": f"{cores * per_core} amplitudes per step on {cores} processes "
                                    "(oracle restatement of scan_plan.sweep_reference, complex128)"},
         "e2e": {"value": value, "unit": "amplitudes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu_kernels": reference_gpu_leg(inst, bits),
     }
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_leg(inst, bits):
+    """The reference's own GPU scan kernels (K2 complex64, K3 complex128; compiled from its
+    source into oracle/_ref/ by oracle/build_ref_gpu.py) driven as its GPUMixin._sweep does,
+    on this box: the bench instance (n = 40) and the reference's RGS70 instance with its
+    frozen order.  Reported beside the CPU arm; `value` stays the CPU executor's rate."""
+    try:
+        import torch
+        from oracle import ref_gpu
+        from oracle import scan_plan as sp
+        if not torch.cuda.is_available():
+            return {"unavailable": "no GPU"}
+        if not (ref_gpu.available("c64") and ref_gpu.available("c128")):
+            return {"unavailable": "oracle/_ref not built (needs the reference checkout at build time)"}
+        out = {"driver": "one string per sweep, one launch per position, host read of the maximum after "
+                         "every launch (GPUMixin._sweep)"}
+        sample = bits[:8]
+        ref_amp = [sp.amplitude(inst.g, inst.u, inst.order, b.tolist()) for b in sample[:2]]
+        for prec in ("c64", "c128"):
+            eng = ref_gpu.RefGpuScan(inst.g, inst.u, inst.order, precision=prec)
+            eng.amplitude(sample[0])
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            amps = [eng.amplitude(b) for b in sample]
+            dt = time.perf_counter() - t0
+            p_ref = np.abs(np.array(ref_amp)) ** 2
+            err = float(np.max(np.abs(np.abs(np.array(amps[:2])) ** 2 - p_ref) / p_ref))
+            out[f"n40_{prec}"] = {"amplitudes_per_s": len(sample) / dt, "strings": len(sample),
+                                  "max_rel_err_vs_oracle": err}
+            del eng
+            torch.cuda.empty_cache()
+        fx = np.load(ROOT / "tests" / "golden" / "fixtures.npz")
+        rec = json.loads((ROOT / "tests" / "golden" / "rgs70_c128.json").read_text())["benchmark_rows"][:2]
+        rbits = np.array([[int(c) for c in r["bitstring_q0_left"]] for r in rec], dtype=np.uint8)
+        rp = np.array([r["probability_c128"] for r in rec])
+        for prec in ("c64", "c128"):
+            eng = ref_gpu.RefGpuScan(fx["rgs70/graph"], fx["rgs70/measurement_unitaries"],
+                                     fx["rgs70/scan_order"].tolist(), precision=prec)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            amps = np.array([eng.amplitude(b) for b in rbits])
+            dt = time.perf_counter() - t0
+            out[f"rgs70_frozen_{prec}"] = {"amplitudes_per_s": len(rbits) / dt, "strings": len(rbits),
+                                           "max_rel_err_vs_reference_records":
+                                               float(np.max(np.abs(np.abs(amps) ** 2 - rp) / rp))}
+            del eng
+            torch.cuda.empty_cache()
+        return out
+    except Exception as exc:  # the CPU arm's line must still print
+        return {"unavailable": f"{type(exc).__name__}: {exc}"}
+
+
+def wht_precision_leg(pkg, device, peak, m=30, m_err=20):
+    """Config 2's WHT variants: the full Walsh-Hadamard transform of a 2^m complex64 state
+    by FP32 butterflies vs 16 x 16 Hadamard blocks on the tensor cores over split-BF16
+    values (2 and 3 terms): time per transform (CUDA events, state of 8 GiB at m = 30:
+    larger than L2), the achieved HBM rate on 16 bytes per element per pass, the relative
+    L2 difference from the FP32 result at m, and the relative L2 error against an FP64
+    transform at m_err."""
+    import torch
+    stream = torch.cuda.current_stream(device)
+    out = {"m": m, "bytes_per_element_per_pass": 16}
+    rng = np.random.default_rng(30)
+    x0 = torch.randn(1 << m, dtype=torch.complex64, device=device)
+    ref32 = None
+    for prec, passes in (("fp32", None), ("split_bf16x2", None), ("split_bf16x3", None)):
+        x = x0.clone()
+        pkg.fwht(x, precision=prec)  # warm-up
+        x.copy_(x0)
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        pkg.fwht(x, precision=prec)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        t = e0.elapsed_time(e1) / 1e3
+        npass = 3 if prec == "fp32" else 1 + math.ceil((m - 12) / 8)
+        rec = {"ms": 1e3 * t, "passes": npass,
+               "achieved_GBps": 16 * npass * (1 << m) / t / 1e9}
+        rec["hbm_frac"] = rec["achieved_GBps"] / peak
+        if prec == "fp32":
+            ref32 = x
+        else:
+            rec["rel_l2_vs_fp32"] = float(torch.linalg.vector_norm(x - ref32) / torch.linalg.vector_norm(ref32))
+            del x
+        out[prec] = rec
+    del ref32, x0
+    torch.cuda.empty_cache()
+    xs = (rng.standard_normal(1 << m_err) + 1j * rng.standard_normal(1 << m_err)).astype(np.complex64)
+    ref = xs.astype(np.complex128)
+    for q in range(m_err):
+        v = ref.reshape(-1, 2, 1 << q)
+        ref = np.stack([v[:, 0] + v[:, 1], v[:, 0] - v[:, 1]], axis=1).reshape(-1)
+    for prec in ("fp32", "split_bf16x2", "split_bf16x3"):
+        d = torch.from_numpy(xs.copy()).to(device)
+        pkg.fwht(d, precision=prec)
+        got = d.cpu().numpy().astype(np.complex128)
+        out[prec][f"rel_l2_err_vs_fp64_m{m_err}"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    return out
 
 
 def run_ours(args, rank, world, local_rank):
@@ -353,6 +471,25 @@ def run_ours(args, rank, world, local_rank):
     globals()["BATCH"] = min(BATCH, 16384)
     chain = run_chain(args, rank, world, local_rank, emit=False)
     globals()["BATCH"] = saved
+    # The other configurations' headline numbers, bounded (single-GPU measurements, rank 0).
+    extra = {}
+    if rank == 0 and not args.no_extra:
+        peak_extra = 6650.0
+        if (ROOT / "MEASURED_PEAKS.json").exists():
+            peak_extra = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"])
+        del graphs
+        torch.cuda.empty_cache()
+        fs, fs_inst = full_scale(pkg, device, 64, legs=("random_order",), rescore=64)
+        leg = fs["random_order"]
+        extra["full_scale_n70"] = dict(leg, workload="config 5: n=70 random degree<=3 graph, seeded random order "
+                                                     f"(r_max {leg['rmax']}), 64 exact Born samples by the chain rule",
+                                       instance=fs_inst.name, unit="samples/s",
+                                       hbm_frac=leg["achieved_GBps"] / peak_extra)
+        torch.cuda.empty_cache()
+        extra["learned_n56"] = learned_comparison(pkg, device, 1024, 1 << 16, 4)
+        torch.cuda.empty_cache()
+        extra["wht_fp32_vs_split_bf16"] = wht_precision_leg(pkg, device, peak_extra)
+        torch.cuda.empty_cache()
     line = None
     if rank == 0:
         cpu = None
@@ -369,7 +506,8 @@ def run_ours(args, rank, world, local_rank):
             "metric": "amplitudes_per_s (p(x), n=40 3-regular, complex64 + FP64 recheck)",
             "value": value, "unit": "amplitudes/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_step / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": ("c64 (fp32 math) + c128 recheck" if args.bulk == "c64f32" else "c64 (fp64 math) + c128 recheck"),
             "data": "synthetic (seeded graph, gates and bitstrings)",
             "config": {"workload": "single-instance throughput: n=40 random 3-regular, Haar SU(2), "
                                    "65536 uniform 40-bit strings, complex64 + FP64 recheck of every result",
@@ -399,6 +537,7 @@ def run_ours(args, rank, world, local_rank):
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
+            **extra,
         }
     if world > 1:
         dist.barrier()
@@ -819,65 +958,77 @@ def run_rgs70(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def full_scale(pkg, device, S, legs=("random_order", "searched_order"), rescore=256, seed=7000):
+    """Config 5, full scale on one GPU: n = 70 random degree-<=3 graph, Haar SU(2) gates, the
+    seeded random order whose max rank is closest to 30 (two complex64 2^30 tables per
+    sample and batch item); S exact Born samples by the chain rule (complex64 tables, float64
+    branch masses), `rescore` of them rescored in complex128, linear XEB with the rescored
+    p and over all samples; optionally the same instance with the package's order search.
+    Returns (legs dict, instance)."""
+    import torch
+    inst = pkg.instances.make_instance("deg3", 70, 70, pkg.rank_profile, target_rank=30,
+                                       order_seeds=range(1000, 1256))
+    edges = pkg.edges_from_graph(inst.g)
+    orders = {"random_order": inst.order}
+    if "searched_order" in legs:
+        orders["searched_order"], _, _ = pkg.search_order(70, edges, inst.order, iterations=200000, seed=1,
+                                                          threads=max(1, min(16, host_cores())))
+    stream = torch.cuda.current_stream(device)
+    raw = {}
+    for name in legs:
+        order = orders[name]
+        plan = pkg.ScanPlan(70, edges, order)
+        tile = 1
+        while tile < 128 and 2 * (2 * tile) * 8 * (1 << plan.rmax) <= 120 * 2 ** 30 and 2 * tile <= S:
+            tile *= 2
+        cs = pkg.ChainSampler(inst.g, inst.u, order, device=device, precision="c64", batch_tile=tile, plan=plan)
+        cs.sample_device(min(S, tile), seed=1, check=True, stream=stream)  # warm-up
+        outs = cs._outs(S)
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        bits, value, logscale, logp = cs.sample_device(S, seed=seed, check=False, stream=stream, outs=outs)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        t = e0.elapsed_time(e1) / 1e3
+        raw[name] = {"samples_per_s": S / t, "seconds": t, "rmax": plan.rmax, "sum_states": plan.sum_states,
+                     "batch_tile": tile, "achieved_GBps": chain_bytes(plan, 8) * S / t / 1e9,
+                     "samples": pkg.unpack_bits(bits.cpu().numpy(), 70),
+                     "p64": np.abs(pkg.amplitudes_from(value.cpu().numpy().astype(np.complex128),
+                                                       logscale.cpu().numpy(), 70)) ** 2,
+                     "logp": logp.cpu().numpy()}
+        del cs, outs, bits, value, logscale, logp
+        torch.cuda.synchronize(device)
+        torch.cuda.empty_cache()
+    # complex128 rescoring with the cheapest order at hand (any order gives the same p(x)).
+    rescore_order = orders.get("searched_order", inst.order)
+    so = pkg.ScanOracle(inst.g, inst.u, rescore_order, device=device, fp64=True)
+    out = {}
+    for name, leg in raw.items():
+        k = min(rescore, S)
+        p128 = so.probabilities(leg["samples"][:k])
+        rel = np.abs(leg["p64"][:k] - p128) / p128
+        out[name] = {key: leg[key] for key in ("samples_per_s", "seconds", "rmax", "sum_states", "batch_tile",
+                                               "achieved_GBps")}
+        out[name].update({"samples": S, "rescored": k, "max_rel_err_c64_vs_c128": float(rel.max()),
+                          "max_abs_logp_minus_log_p128": float(np.max(np.abs(leg["logp"][:k] - np.log(p128)))),
+                          "linear_xeb_rescored": float((2.0 ** 70) * p128.mean() - 1),
+                          "linear_xeb_all_c64": float((2.0 ** 70) * leg["p64"].mean() - 1)})
+    del so
+    torch.cuda.empty_cache()
+    return out, inst
+
+
 def run_full(args, rank, world, local_rank):
-    """Full scale on one GPU: n = 70 random degree-<=3 graph, Haar SU(2) gates, the seeded
-    random order whose max rank is closest to 30 (two complex64 2^30 tables per sample);
-    `--samples` exact Born samples by the chain rule (complex64 tables, float64 branch
-    masses), 256 of them rescored in complex128, linear XEB with the rescored p.  Then the
-    same instance with the order from the package's order search."""
+    """Full scale on one GPU (config 5) with `--samples` exact samples, random and searched orders."""
     import torch
     import __graft_entry__
     pkg = __graft_entry__.package()
     device = torch.device("cuda", local_rank)
     torch.cuda.set_device(device)
-    inst = pkg.instances.make_instance("deg3", 70, 70, pkg.rank_profile, target_rank=30,
-                                       order_seeds=range(1000, 1256))
-    edges = pkg.edges_from_graph(inst.g)
-    searched, _, _ = pkg.search_order(70, edges, inst.order, iterations=200000, seed=1,
-                                      threads=max(1, min(16, host_cores())))
-    stream = torch.cuda.current_stream(device)
     S = args.samples
-    legs = {}
     with ClockSampler(local_rank) as clocks:
-        for name, order in (("random_order", inst.order), ("searched_order", searched)):
-            plan = pkg.ScanPlan(70, edges, order)
-            tile = 1
-            while tile < 128 and 2 * (2 * tile) * 8 * (1 << plan.rmax) <= 120 * 2 ** 30:
-                tile *= 2
-            cs = pkg.ChainSampler(inst.g, inst.u, order, device=device, precision="c64", batch_tile=tile, plan=plan)
-            cs.sample_device(min(S, tile), seed=1, check=True, stream=stream)  # warm-up
-            outs = cs._outs(S)
-            torch.cuda.synchronize(device)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            bits, value, logscale, logp = cs.sample_device(S, seed=7000 + rank, check=False, stream=stream, outs=outs)
-            e1.record(stream)
-            torch.cuda.synchronize(device)
-            t = e0.elapsed_time(e1) / 1e3
-            samples = pkg.unpack_bits(bits.cpu().numpy(), 70)
-            p64 = np.abs(pkg.amplitudes_from(value.cpu().numpy().astype(np.complex128), logscale.cpu().numpy(),
-                                             70)) ** 2
-            lp = logp.cpu().numpy()
-            legs[name] = {"samples_per_s": S / t, "seconds": t, "rmax": plan.rmax, "sum_states": plan.sum_states,
-                          "batch_tile": tile, "achieved_GBps": chain_bytes(plan, 8) * S / t / 1e9,
-                          "samples": samples, "p64": p64, "logp": lp}
-            del cs, outs, bits, value, logscale, logp
-            torch.cuda.synchronize(device)
-            torch.cuda.empty_cache()
-    # complex128 rescoring of 256 samples of each leg with the searched order (any order
-    # gives the same p(x); the searched one is cheap).
-    so = pkg.ScanOracle(inst.g, inst.u, searched, device=device, fp64=True)
-    out = {}
-    for name, leg in legs.items():
-        k = min(256, S)
-        p128 = so.probabilities(leg["samples"][:k])
-        rel = np.abs(leg["p64"][:k] - p128) / p128
-        out[name] = {key: leg[key] for key in ("samples_per_s", "seconds", "rmax", "sum_states", "batch_tile",
-                                               "achieved_GBps")}
-        out[name].update({"rescored": k, "max_rel_err_c64_vs_c128": float(rel.max()),
-                          "max_abs_logp_minus_log_p128": float(np.max(np.abs(leg["logp"][:k] - np.log(p128)))),
-                          "linear_xeb_rescored": float((2.0 ** 70) * p128.mean() - 1),
-                          "linear_xeb_all_c64": float((2.0 ** 70) * leg["p64"].mean() - 1)})
+        out, inst = full_scale(pkg, device, S, seed=7000 + rank)
     peaks_path = ROOT / "MEASURED_PEAKS.json"
     peak = float(json.loads(peaks_path.read_text())["hbm_gbs"]) if peaks_path.exists() else 6650.0
     main = out["random_order"]
@@ -895,42 +1046,44 @@ def run_full(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
-def run_learned(args, rank, world, local_rank):
-    """Learned proposal workload: n=56 random degree<=3 graph (seeded order, max rank <= 28),
-    MADE 2x512 trained on 2^16 exact samples + their exact conditionals; 4096 samples from
-    (a) rejection with the learned proposal (Born-exact under the calibrated envelope),
-    (b) the plain exact sampler (chain rule over the scan), (c) the reference's uniform
-    capped rule (cap 1, not Born)."""
+def learned_comparison(pkg, device, samples, train_samples, epochs, order_policy="searched", batch_tile=64):
+    """Config 4: n=56 random degree<=3 graph (max rank <= 28), MADE 2x512 trained on exact
+    samples + their exact conditionals; `samples` accepted samples from (a) rejection with
+    the learned proposal (Born-exact under the calibrated envelope), (b) the plain exact
+    sampler (chain rule over the scan), (c) the reference's uniform capped rule (cap 1, not
+    Born).  order_policy "searched": the package's order search from the seeded order;
+    "random": the seeded random order.  Returns a dict of measurements."""
     import torch
-    import __graft_entry__
-    pkg = __graft_entry__.package()
-    device = torch.device("cuda", local_rank)
-    torch.cuda.set_device(device)
-    n, target = 56, args.samples
+    n = 56
     inst = pkg.instances.make_instance("deg3", n, 56, pkg.rank_profile)
-    if inst.rmax > 28:
-        raise SystemExit(f"instance rank {inst.rmax} above 28")
-    cs = pkg.ChainSampler(inst.g, inst.u, inst.order, device=device, precision="c64", batch_tile=64)
-    so = pkg.ScanOracle(inst.g, inst.u, inst.order, device=device, batch_tile=64)
-    so128 = pkg.ScanOracle(inst.g, inst.u, inst.order, device=device, fp64=True, batch_tile=32)
-    order = np.asarray(inst.order)
-    inv = np.argsort(order)
+    order = inst.order
+    if order_policy == "searched":
+        order, _, _ = pkg.search_order(n, pkg.edges_from_graph(inst.g), inst.order, iterations=100000, seed=1,
+                                       threads=max(1, min(16, host_cores())))
+    plan = pkg.ScanPlan(n, pkg.edges_from_graph(inst.g), order)
+    if plan.rmax > 28:
+        raise SystemExit(f"instance rank {plan.rmax} above 28")
+    cs = pkg.ChainSampler(inst.g, inst.u, order, device=device, precision="c64", batch_tile=batch_tile)
+    so = pkg.ScanOracle(inst.g, inst.u, order, device=device, precision="c64f32")
+    so128 = pkg.ScanOracle(inst.g, inst.u, order, device=device, fp64=True)
+    order_a = np.asarray(order)
+    inv = np.argsort(order_a)
     t0 = time.perf_counter()
-    bits, p, logp, cond = cs.sample(1 << 16, seed=1, with_conditionals=True)
+    bits, p, logp, cond = cs.sample(train_samples, seed=1, with_conditionals=True)
     t_data = time.perf_counter() - t0
     net = pkg.MadeProposal(n, hidden=512, device=device, seed=3)
     t0 = time.perf_counter()
-    losses = net.fit(bits[:, order], cond, epochs=args.epochs, batch=4096, lr=3e-3)
+    losses = net.fit(bits[:, order_a], cond, epochs=epochs, batch=4096, lr=3e-3)
     torch.cuda.synchronize(device)
     t_train = time.perf_counter() - t0
     c = np.clip(cond.astype(np.float64), 1e-12, 1 - 1e-12)
     floor = float(np.mean(np.sum(-(c * np.log(c) + (1 - c) * np.log(1 - c)), axis=1)))
     # Envelope from held-out exact samples; deficit (TV of the output) on a separate set.
     cal_bits, _, cal_logp = cs.sample(16384, seed=2)
-    cal_lq = net.log_q(torch.as_tensor(cal_bits[:, order].astype(np.float32)).to(device)).cpu().numpy()
+    cal_lq = net.log_q(torch.as_tensor(cal_bits[:, order_a].astype(np.float32)).to(device)).cpu().numpy()
     log_c, _ = pkg.calibrate_envelope(cal_logp, cal_lq, quantile=1.0, slack=1.5)
     val_bits, _, val_logp = cs.sample(16384, seed=3)
-    val_lq = net.log_q(torch.as_tensor(val_bits[:, order].astype(np.float32)).to(device)).cpu().numpy()
+    val_lq = net.log_q(torch.as_tensor(val_bits[:, order_a].astype(np.float32)).to(device)).cpu().numpy()
     deficit = float(np.mean(np.maximum(0.0, 1.0 - np.exp(log_c - (val_logp - val_lq)))))
     viol_val = int(np.sum(val_logp - val_lq > log_c))
 
@@ -942,43 +1095,54 @@ def run_learned(args, rank, world, local_rank):
     rng = np.random.default_rng(4)
     torch.cuda.synchronize(device)
     t0 = time.perf_counter()
-    lbits, lp, lst = pkg.rejection_sample(so.probabilities, propose, log_c, target, rng,
+    lbits, lp, lst = pkg.rejection_sample(so.probabilities, propose, log_c, samples, rng,
                                           recheck_fn=so128.probabilities)
     torch.cuda.synchronize(device)
     t_learned = time.perf_counter() - t0
     t0 = time.perf_counter()
-    cbits, cp, clogp = cs.sample(target, seed=5)
+    cbits, cp, clogp = cs.sample(samples, seed=5)
     torch.cuda.synchronize(device)
     t_chain = time.perf_counter() - t0
     t0 = time.perf_counter()
-    recs, usum = pkg.capped_rejection(so, np.random.default_rng(314159), target, cap=1.0, recheck=so128,
+    recs, usum = pkg.capped_rejection(so, np.random.default_rng(314159), samples, cap=1.0, recheck=so128,
                                       batch=8192, max_proposals=1 << 22)
     torch.cuda.synchronize(device)
     t_uni = time.perf_counter() - t0
-    learned = target / t_learned
-    chain = target / t_chain
+    learned, chain = samples / t_learned, samples / t_chain
+    return {
+        "workload": f"n=56 random degree<=3 graph, {order_policy} order", "rmax": plan.rmax,
+        "sum_states": plan.sum_states, "samples": samples, "mlp": "MADE 2x512, bf16 tcgen05 GEMMs, fp32 accumulation",
+        "training_samples": train_samples, "epochs": epochs,
+        "learned": {"samples_per_s": learned, "acceptance": lst["acceptance"], "proposals": lst["proposals"],
+                    "linear_xeb": lst["linear_xeb"], "fp64_rechecked": lst["fp64_rechecked"],
+                    "fp64_flips": lst["fp64_flips"], "envelope_violations": lst["envelope_violations"]},
+        "plain_chain_rule": {"samples_per_s": chain, "linear_xeb": float((2.0 ** n) * cp.mean() - 1)},
+        "uniform_capped_reference_rule": {"samples_per_s": samples / t_uni, "acceptance": usum["acceptance_fraction"],
+                                          "xeb": usum["xeb"], "born_exact": False},
+        "learned_over_plain": learned / chain,
+        "envelope": {"log_c": log_c, "validation_deficit_tv": deficit, "validation_violations": viol_val,
+                     "validation_samples": 16384},
+        "training": {"exact_sample_seconds": t_data, "train_seconds": t_train, "loss_first": losses[0],
+                     "loss_last": float(np.mean(losses[-5:])), "entropy_floor": floor,
+                     "kl_estimate": float(np.mean(losses[-5:]) - floor)}}
+
+
+def run_learned(args, rank, world, local_rank):
+    """Learned proposal workload (config 4) at full size: 2^16 training samples, `--samples`
+    accepted samples; `--order random` keeps the seeded random order (rank 25)."""
+    import torch
+    import __graft_entry__
+    pkg = __graft_entry__.package()
+    device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+    res = learned_comparison(pkg, device, args.samples, 1 << 16, args.epochs, order_policy=args.order)
     if rank == 0:
         print(json.dumps({
             "metric": "exact_born_samples_per_s (learned proposal vs plain exact sampler, n=56 degree<=3)",
-            "value": learned, "unit": "samples/s", "n_gpus": 1, "steps": 1, "warmup": 0,
-            "ms_per_step": 1e3 * t_learned, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "c64 scan, bf16 MLP", "data": "synthetic (seeded graph, gates, samples)",
-            "config": {"workload": "n=56 random degree<=3 graph, seeded random order", "rmax": inst.rmax,
-                       "sum_states": inst.sum_states, "samples": target, "mlp": "MADE 2x512 bf16/fp32",
-                       "training_samples": 1 << 16, "epochs": args.epochs},
-            "learned": {"samples_per_s": learned, "acceptance": lst["acceptance"], "proposals": lst["proposals"],
-                        "linear_xeb": lst["linear_xeb"], "fp64_rechecked": lst["fp64_rechecked"],
-                        "fp64_flips": lst["fp64_flips"], "envelope_violations": lst["envelope_violations"]},
-            "plain_chain_rule": {"samples_per_s": chain, "linear_xeb": float((2.0 ** n) * cp.mean() - 1)},
-            "uniform_capped_reference_rule": {"samples_per_s": target / t_uni,
-                                              "acceptance": usum["acceptance_fraction"], "xeb": usum["xeb"],
-                                              "born_exact": False},
-            "learned_over_plain": learned / chain,
-            "envelope": {"log_c": log_c, "validation_deficit_tv": deficit, "validation_violations": viol_val,
-                         "validation_samples": 16384},
-            "training": {"exact_sample_seconds": t_data, "train_seconds": t_train, "loss_first": losses[0],
-                         "loss_last": float(np.mean(losses[-5:])), "entropy_floor": floor,
-                         "kl_estimate": float(np.mean(losses[-5:]) - floor)}}), flush=True)
+            "value": res["learned"]["samples_per_s"], "unit": "samples/s", "n_gpus": 1, "steps": 1, "warmup": 0,
+            "ms_per_step": 1e3 * args.samples / res["learned"]["samples_per_s"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64 scan, bf16 MLP",
+            "data": "synthetic (seeded graph, gates, samples)", "config": res}), flush=True)
 
 
 def main():
@@ -993,9 +1157,13 @@ def main():
     ap.add_argument("--only", choices=["both", "c64", "c128"], default="both",
                     help="run only one precision (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the other configurations' legs of the default line (profiling runs)")
     ap.add_argument("--workload", choices=["amplitudes", "fourier", "chain", "learned", "batched", "rgs70", "full"], default="amplitudes")
     ap.add_argument("--samples", type=int, default=4096, help="learned: accepted samples; full: exact samples")
     ap.add_argument("--epochs", type=int, default=8, help="training epochs of the learned workload")
+    ap.add_argument("--order", choices=["searched", "random"], default="searched",
+                    help="scan order of the learned workload's n=56 instance")
     ap.add_argument("--m", type=int, default=30, help="conditional qubits of the fourier workload")
     ap.add_argument("--tile64", type=int, default=None, help="complex64 batch tile (default: autotuned)")
     ap.add_argument("--bulk", choices=["c64f32", "c64"], default="c64f32",

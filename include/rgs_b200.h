@@ -9,8 +9,8 @@
  *
  * Reference interfaces replaced (whyihaveyou/rgs70-classical-challenge,
  * W/ = work/rgs_attack/) are cited beside each function.  The reference exposes
- * only Python; these are the functions its Python layer would bind (see
- * INTEGRATION.md for the ctypes stubs).
+ * only Python; these are the functions its Python layer would bind through
+ * ctypes.
  *
  * Conventions.  Qubit/vertex q of a bitstring is bit q of a little-endian pair
  * of uint64 words (bits[2*i] holds qubits 0..63, bits[2*i+1] qubits 64..127).
@@ -270,6 +270,15 @@ int rgs_fourier_quadphase(rgs_fourier* plan, void* state, void* stream);
 /* Building blocks on a device complex64 state of 2^nbits values (nbits >= 4), in place. */
 /* Walsh-Hadamard butterflies on bits [lo, hi) (lowfwht/localfwht/fusedfwht). */
 int rgs_fwht(void* state, int32_t nbits, int32_t lo, int32_t hi, void* stream);
+/* The same butterflies with a precision switch: RGS_WHT_FP32 (= rgs_fwht), or 16 x 16
+ * Hadamard blocks on the tensor cores (tcgen05.mma, FP32 accumulation in TMEM) over a
+ * split-BF16 copy of each value with 2 or 3 terms (RGS_WHT_SPLIT_BF16X2: about 4e-6
+ * relative error per 4-bit round, RGS_WHT_SPLIT_BF16X3: FP32 level).  Tensor-core
+ * variants need nbits >= 12 and a 16-byte aligned state. */
+#define RGS_WHT_FP32 0
+#define RGS_WHT_SPLIT_BF16X2 2
+#define RGS_WHT_SPLIT_BF16X3 3
+int rgs_fwht_precision(void* state, int32_t nbits, int32_t lo, int32_t hi, int32_t precision, void* stream);
 /* Per-qubit 2x2 products on bits [lo, hi); unitaries: device complex128[nbits][2][2]
  * (lowprod/localprod/fusedprod). */
 int rgs_product(void* state, int32_t nbits, const double* unitaries, int32_t lo, int32_t hi, void* stream);
@@ -280,12 +289,17 @@ int rgs_block_mass(const void* state, int32_t nbits, int32_t tile_bits, double* 
  * No counterpart in the reference, which proposes uniformly (W/rejection_sampler.py:19);
  * these are the kernels of the masked autoregressive proposal used for rejection
  * sampling against the engine's p(x).  BF16 operands, FP32 accumulation on the tensor
- * cores.  All pointers are device pointers; bf16 arrays are raw 16-bit values. */
+ * cores (tcgen05.mma into TMEM).  All pointers are device pointers; bf16 arrays are raw
+ * 16-bit values. */
 /* C[M][N] = alpha * op(A) op(B) (+ bias[N]) (relu) (* mask[M][N]) (* [gate[M][N] > 0]);
  * A: [M][lda] (transA: [K][lda]); B: [K][ldb] (transB: [N][ldb]); C fp32 and/or Cb bf16. */
 int rgs_gemm_bf16(int32_t M, int32_t N, int32_t K, const void* A, int32_t lda, int32_t transA, const void* B,
                   int32_t ldb, int32_t transB, float alpha, const float* bias, int32_t relu, const uint8_t* mask,
                   const void* gate, float* C, void* Cb, int32_t ldc, void* stream);
+/* *timed_out = 1 if a bounded wait of a tensor-core kernel (GEMM, tensor-core Hadamard
+ * passes) gave up since the last call (its results are then invalid); clears the flag.
+ * Synchronous. */
+int rgs_tensor_core_status(int32_t* timed_out);
 /* Forward: x bf16[batch][n] -> h1, h2 bf16[batch][hidden] -> logits z fp32[batch][n];
  * weights bf16 W1[hidden][n], W2[hidden][hidden], W3[n][hidden] (already masked), biases fp32. */
 int rgs_mlp_fwd(int32_t batch, int32_t n, int32_t hidden, const void* x, const void* w1b, const float* b1,
@@ -313,15 +327,22 @@ int rgs_mlp_logq(int32_t batch, int32_t n, int32_t hidden, const void* x, const 
 
 /* ---------------------------------------------------------------- allocation-free scan
  * No counterpart in the reference.  Same result as rgs_scan_amplitudes, for callers
- * that cannot allocate device memory at call time (host callbacks, hosts that give
- * the library a fixed memory budget, integrations whose allocator must own every
- * byte): no workspace argument, and no cudaMalloc/cudaFree or allocating library
- * call.  All scratch lives in one static device array of RGS_NOALLOC_SCRATCH_BYTES
- * (64 MiB) per GPU, held from library load until process exit; plans whose scratch
- * does not fit (complex64 rank above about 21) are rejected with RGS_ERR_OOM.  The
- * first call on a device looks up the array's address (make it before any stream
- * capture).  Calls share the array: calls that overlap on the GPU race, so serialise
- * them.  out_value: complex64[batch] or complex128[batch] (RGS_PREC_C128). */
+ * that cannot let the library allocate device memory: hosts that give it a fixed
+ * device-memory budget, and integrations whose own allocator must own every byte of
+ * the GPU.  No workspace argument, and no cudaMalloc/cudaFree or allocating library
+ * call: all scratch lives in one static device array of RGS_NOALLOC_SCRATCH_BYTES
+ * (64 MiB) per GPU, held from library load until process exit.  It must hold the
+ * plan's per-step byte tables plus one batch tile's two environment tables; plans
+ * whose scratch does not fit at batch tile 1 (complex64 rank above about 21,
+ * complex128 above about 20) are rejected with RGS_ERR_OOM.  "No allocation" means
+ * no device allocation only: the call still makes CUDA runtime calls, takes a host
+ * mutex and builds small host vectors, so never call it from a CUDA host callback
+ * (cudaLaunchHostFunc) or a signal handler.  The first call on a device looks up the
+ * array's address and caches it for the process; do not use the library on a device
+ * after cudaDeviceReset.  Every call uploads the plan's tables from pageable host
+ * memory, so a call on a stream that is being captured returns RGS_ERR_UNSUPPORTED.
+ * Calls share the array: calls that overlap on the GPU race, so serialise them.
+ * out_value: complex64[batch] or complex128[batch] (RGS_PREC_C128). */
 #define RGS_NOALLOC_SCRATCH_BYTES (64ull << 20)
 int rgs_scan_amplitudes_noalloc(rgs_plan* plan, const double* unitaries, const uint64_t* bits, int64_t batch,
                                 int32_t precision, void* out_value, double* out_logscale, void* stream);

@@ -105,6 +105,7 @@ SIGNATURES = {
                                      ctypes.c_int32, c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_float,
                                      c_void_p, ctypes.c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
                                      ctypes.c_int32, c_void_p]),
+    "rgs_tensor_core_status": (ctypes.c_int, [c_int32_p]),
     "rgs_mlp_fwd": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32] + [c_void_p] * 11),
     "rgs_mlp_bwd": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32] + [c_void_p] * 20
                     + [ctypes.c_int32, c_void_p]),
@@ -132,6 +133,8 @@ SIGNATURES = {
     "rgs_fourier_index_map": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "rgs_fourier_quadphase": (ctypes.c_int, [c_void_p, c_void_p, c_void_p]),
     "rgs_fwht": (ctypes.c_int, [c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_void_p]),
+    "rgs_fwht_precision": (ctypes.c_int, [c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                          c_void_p]),
     "rgs_product": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_void_p, ctypes.c_int32, ctypes.c_int32, c_void_p]),
     "rgs_block_mass": (ctypes.c_int, [c_void_p, ctypes.c_int32, ctypes.c_int32, c_void_p, c_void_p]),
 }

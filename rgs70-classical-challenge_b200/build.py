@@ -20,6 +20,8 @@ LIB = PKG / "librgs_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
          "-I", str(CSRC), "-I", str(INCLUDE)]
+# Extra nvcc flags (launch-shape knobs such as -DRGS_PAIR_MINB=3 for tuning builds).
+FLAGS += os.environ.get("RGS_NVCC_FLAGS", "").split()
 
 
 def _nvcc():

@@ -140,6 +140,13 @@ int rgs_fwht(void* state, int32_t nbits, int32_t lo, int32_t hi, void* stream) {
   return fwht_bits(state, nbits, lo, hi, (cudaStream_t)stream);
 }
 
+int rgs_fwht_precision(void* state, int32_t nbits, int32_t lo, int32_t hi, int32_t precision, void* stream) {
+  if (precision == RGS_WHT_FP32) return fwht_bits(state, nbits, lo, hi, (cudaStream_t)stream);
+  if (precision == RGS_WHT_SPLIT_BF16X2 || precision == RGS_WHT_SPLIT_BF16X3)
+    return fwht_tensor_core(state, nbits, lo, hi, precision, (cudaStream_t)stream);
+  return fail(RGS_ERR_ARG, "unknown WHT precision");
+}
+
 int rgs_product(void* state, int32_t nbits, const double* unitaries, int32_t lo, int32_t hi, void* stream) {
   return product_bits(state, nbits, unitaries, lo, hi, (cudaStream_t)stream);
 }

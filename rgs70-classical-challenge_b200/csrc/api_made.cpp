@@ -74,6 +74,14 @@ int rgs_gemm_bf16(int32_t M, int32_t N, int32_t K, const void* A, int32_t lda, i
   return gemm_bf16(g, (cudaStream_t)stream);
 }
 
+int rgs_tensor_core_status(int32_t* timed_out) {
+  if (!timed_out) return fail(RGS_ERR_ARG, "timed_out is NULL");
+  int v = 0;
+  int rc = tensor_core_status(&v);
+  *timed_out = v;
+  return rc;
+}
+
 int rgs_mlp_fwd(int32_t batch, int32_t n, int32_t hidden, const void* x, const void* w1b, const float* b1,
                 const void* w2b, const float* b2, const void* w3b, const float* b3, void* h1b, void* h2b, float* z,
                 void* stream) {

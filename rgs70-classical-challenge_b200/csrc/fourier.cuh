@@ -106,6 +106,9 @@ int fourier_quadphase(FourierPlan& p, void* state, cudaStream_t s);
 
 // Building blocks on a state of 2^nbits complex64 values (in place).
 int fwht_bits(void* state, int nbits, int lo, int hi, cudaStream_t s);
+// The same butterflies with 16 x 16 Hadamard blocks on the tensor cores over `terms` (2
+// or 3) BF16 parts of each value (wht_tc.cu); nbits >= 12.
+int fwht_tensor_core(void* state, int nbits, int lo, int hi, int terms, cudaStream_t s);
 int product_bits(void* state, int nbits, const double* u_host, int lo, int hi, cudaStream_t s);
 int block_mass(const void* state, int nbits, int tile_bits, double* masses, cudaStream_t s);
 

@@ -1,14 +1,12 @@
 // Masked autoregressive proposal network (MADE, Germain et al. 2015): BF16 GEMMs with
-// FP32 accumulation on the tensor cores (mma.sync m16n8k16), fused epilogues, and the
-// loss / gradient / Adam kernels of its training.
+// FP32 accumulation on the Blackwell tensor cores (tcgen05.mma, accumulators in TMEM),
+// fused epilogues, and the loss / gradient / Adam kernels of its training.
 //
 // Network: x in {0,1}^n (scan order) -> h1 = relu((W1*M1) x + b1) -> h2 = relu((W2*M2) h1
 // + b2) -> z = (W3*M3) h2 + b3, q(x_d = 1 | x_<d) = sigmoid(z_d).  Masks M1..M3 enforce
 // the autoregressive order; the masked weights are kept as BF16 copies for the GEMMs and
-// as FP32 masters for the optimiser.
-//
-// The network is a few percent of a sample's cost next to the scan, so its GEMMs use the
-// warp-level MMA; everything stays on the device (no host round trips per step).
+// as FP32 masters for the optimiser.  Everything stays on the device (no host round
+// trips per step).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -16,90 +14,159 @@
 
 #include "common.hpp"
 #include "made.hpp"
+#include "tcgen05.cuh"
 
 namespace rgs {
 
+// Set when a bounded wait of this file's GEMM gave up (read by tensor_core_status).
+__device__ int g_tc_timeout = 0;
+
+int wht_tensor_core_timeout(int* timed_out);
+
 namespace {
 
-constexpr int BM = 64, BN = 64, BK = 32, PADK = 8;
+// CTA tile of the tensor-core GEMM: 128 x 128 outputs (one TMEM accumulator of 128 lanes
+// x 128 fp32 columns), K in slices of 64, two shared-memory stages.
+constexpr int TBM = 128, TBN = 128, TBK = 64, kStages = 2;
+constexpr int kTileBytes = TBM * TBK * 2;  // one 128 x 64 bf16 operand tile (16 KiB)
+constexpr int kGemmSmem = kStages * 2 * kTileBytes + 1024 + 64;
 
-__device__ __forceinline__ unsigned pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi) {
-  return (unsigned)__bfloat16_as_ushort(lo) | ((unsigned)__bfloat16_as_ushort(hi) << 16);
+// Byte offset of the 16-byte chunk (row r, k-chunk kc) of a 128 x 64 operand tile in the
+// K-major no-swizzle layout: core matrices of 8 rows x 16 bytes, the eight k-chunks of a
+// row group 128 bytes apart (LBO), row groups 1024 bytes apart (SBO).
+__device__ __forceinline__ uint32_t cm_off(int r, int kc) { return (uint32_t)((r >> 3) * 1024 + kc * 128 + (r & 7) * 16); }
+
+__device__ __forceinline__ unsigned bf_bits(const __nv_bfloat16* p) { return (unsigned)__bfloat16_as_ushort(*p); }
+
+__device__ __forceinline__ unsigned word_of(const uint4& v, int w) {
+  return w == 0 ? v.x : (w == 1 ? v.y : (w == 2 ? v.z : v.w));
 }
 
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+// Eight consecutive bf16 values, those at index >= valid replaced by zero.
+__device__ __forceinline__ uint4 load8_partial(const __nv_bfloat16* src, int valid) {
+  unsigned w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+    if (j < valid) w[j >> 1] |= bf_bits(src + j) << (16 * (j & 1));
+  return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// Rows [r0, r0 + 128) x k [k0, k0 + 64) of a logical R x K operand into the K-major
+// layout; zero outside the operand.  kmajor: element (r, k) at G[r * ld + k]; otherwise
+// at G[k * ld + r] (MN-major: transposed in registers on the way).  128 threads, one
+// 8 x 8 core matrix each; vec: 16-byte loads are aligned (ld % 8 == 0, G 16-byte aligned).
+__device__ __forceinline__ void stage_tile(unsigned char* tile, const __nv_bfloat16* __restrict__ G, int ld, int R,
+                                           int K, int r0, int k0, bool kmajor, bool vec) {
+  const int t = threadIdx.x;
+  if (kmajor) {
+    const int kc = t & 7, rg = t >> 3;
+    const int k = k0 + kc * 8;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int ii = (i + kc) & 7;  // rotated so that a quarter warp hits distinct banks
+      const int r = r0 + rg * 8 + ii;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (r < R && k < K) {
+        const __nv_bfloat16* src = G + (size_t)r * ld + k;
+        v = (vec && k + 8 <= K) ? __ldg(reinterpret_cast<const uint4*>(src)) : load8_partial(src, K - k);
+      }
+      *reinterpret_cast<uint4*>(tile + cm_off(rg * 8 + ii, kc)) = v;
+    }
+  } else {
+    const int rg = t & 15, kc = t >> 4;
+    const int r = r0 + rg * 8;
+    uint4 rows[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int k = k0 + kc * 8 + j;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (k < K && r < R) {
+        const __nv_bfloat16* src = G + (size_t)k * ld + r;
+        v = (vec && r + 8 <= R) ? __ldg(reinterpret_cast<const uint4*>(src)) : load8_partial(src, R - r);
+      }
+      rows[j] = v;
+    }
+    // Row e of the core matrix = element e of the eight loaded k-rows.
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int e = (i + rg) & 7;
+      const unsigned sel = (e & 1) ? 0x7632u : 0x5410u;
+      unsigned w[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const unsigned a = word_of(rows[2 * j], e >> 1), b = word_of(rows[2 * j + 1], e >> 1);
+        w[j] = __byte_perm(a, b, sel);
+      }
+      *reinterpret_cast<uint4*>(tile + cm_off(rg * 8 + e, kc)) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+  }
 }
 
 // C[M x N] = op(A)[M x K] * op(B)[K x N]; A row-major [M][lda] (transA: [K][lda]), B
-// row-major [K][ldb] (transB: [N][ldb]).  128 threads: 4 warps in a 2x2 grid of 32x32.
-__global__ void __launch_bounds__(128) gemm_bf16_kernel(GemmArgs g) {
-  __shared__ __nv_bfloat16 As[BM][BK + PADK];
-  __shared__ __nv_bfloat16 Bs[BN][BK + PADK];
-  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+// row-major [K][ldb] (transB: [N][ldb]).  One CTA of 128 threads per 128 x 128 tile of C:
+// all threads stage a K-slice of both operands (double-buffered), thread 0 issues four
+// tcgen05.mma (K = 16 each) per slice into the TMEM accumulator and commits them to the
+// stage's mbarrier, which gates the reuse of that stage; after the last slice every warp
+// reads its 32 TMEM lanes (rows) and applies the epilogue.
+__global__ void __launch_bounds__(128) gemm_tc_kernel(GemmArgs g) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kStages * 2 * kTileBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kStages);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  const int grp = lane >> 2, tig = lane & 3;
-  float acc[2][4][4];
-  for (int i = 0; i < 2; ++i)
-    for (int j = 0; j < 4; ++j)
-      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
-  const __nv_bfloat16 zero = __float2bfloat16(0.f);
-  for (int k0 = 0; k0 < g.K; k0 += BK) {
-    for (int idx = threadIdx.x; idx < BM * BK; idx += blockDim.x) {
-      const int r = idx / BK, c = idx % BK;  // (m, k) of the tile
-      const int m = m0 + r, k = k0 + c;
-      __nv_bfloat16 v = zero;
-      if (m < g.M && k < g.K) v = g.transA ? g.A[(size_t)k * g.lda + m] : g.A[(size_t)m * g.lda + k];
-      As[r][c] = v;
-    }
-    for (int idx = threadIdx.x; idx < BN * BK; idx += blockDim.x) {
-      const int r = idx / BK, c = idx % BK;  // (n, k) of the tile
-      const int n = n0 + r, k = k0 + c;
-      __nv_bfloat16 v = zero;
-      if (n < g.N && k < g.K) v = g.transB ? g.B[(size_t)n * g.ldb + k] : g.B[(size_t)k * g.ldb + n];
-      Bs[r][c] = v;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < BK; kk += 16) {
-      unsigned a[2][4], b[4][2];
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const int r = wm + i * 16 + grp;
-        a[i][0] = pack_bf16(As[r][kk + tig * 2], As[r][kk + tig * 2 + 1]);
-        a[i][1] = pack_bf16(As[r + 8][kk + tig * 2], As[r + 8][kk + tig * 2 + 1]);
-        a[i][2] = pack_bf16(As[r][kk + tig * 2 + 8], As[r][kk + tig * 2 + 9]);
-        a[i][3] = pack_bf16(As[r + 8][kk + tig * 2 + 8], As[r + 8][kk + tig * 2 + 9]);
-      }
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int c = wn + j * 8 + grp;
-        b[j][0] = pack_bf16(Bs[c][kk + tig * 2], Bs[c][kk + tig * 2 + 1]);
-        b[j][1] = pack_bf16(Bs[c][kk + tig * 2 + 8], Bs[c][kk + tig * 2 + 9]);
-      }
-#pragma unroll
-      for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) mma_bf16(acc[i][j], a[i], b[j]);
-    }
-    __syncthreads();
+  const int m0 = blockIdx.y * TBM, n0 = blockIdx.x * TBN;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) tc::mbar_init(&bars[s], 1);
+    tc::fence_barrier_init();
   }
-  // Epilogue: + bias[n], relu, * mask[m][n], * (gate[m][n] > 0); fp32 and/or bf16 out.
+  if (warp == 0) tc::tmem_alloc(tmem_slot, TBN);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tmem_slot;
+  const bool vecA = (g.lda % 8 == 0) && (((uintptr_t)g.A & 15) == 0);
+  const bool vecB = (g.ldb % 8 == 0) && (((uintptr_t)g.B & 15) == 0);
+  const int KT = (g.K + TBK - 1) / TBK;
+  const uint32_t idesc = tc::instr_desc(TBM, TBN, 1);
+  bool ok = true;
+  for (int kt = 0; kt < KT; ++kt) {
+    const int s = kt & 1;
+    if (kt >= kStages && !tc::mbar_wait(&bars[s], (uint32_t)((kt >> 1) - 1) & 1u)) ok = false;
+    if (!__syncthreads_and(ok)) {
+      ok = false;
+      break;
+    }
+    unsigned char* As = base + s * 2 * kTileBytes;
+    unsigned char* Bs = As + kTileBytes;
+    stage_tile(As, g.A, g.lda, g.M, g.K, m0, kt * TBK, !g.transA, vecA);
+    stage_tile(Bs, g.B, g.ldb, g.N, g.K, n0, kt * TBK, g.transB != 0, vecB);
+    tc::fence_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tc::fence_after_sync();
+      const uint32_t a0 = tc::smem_u32(As), b0 = tc::smem_u32(Bs);
 #pragma unroll
-  for (int i = 0; i < 2; ++i)
+      for (int k = 0; k < TBK / 16; ++k)
+        tc::mma_f16(tmem, tc::smem_desc(a0 + k * 256, 128, 1024, 0), tc::smem_desc(b0 + k * 256, 128, 1024, 0), idesc,
+                    (kt > 0 || k > 0) ? 1u : 0u);
+      tc::mma_commit(&bars[s]);
+    }
+  }
+  if (ok && KT > 0 && !tc::mbar_wait(&bars[(KT - 1) & 1], (uint32_t)((KT - 1) >> 1) & 1u)) ok = false;
+  ok = __syncthreads_and(ok);
+  tc::fence_after_sync();
+  if (ok) {
+    const int m = m0 + warp * 32 + lane;
+    for (int c0 = 0; c0 < TBN && n0 + c0 < g.N; c0 += 16) {
+      uint32_t r[16];
+      tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
+      tc::tmem_ld_wait();
+      if (m >= g.M) continue;
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int m = m0 + wm + i * 16 + grp + (e >= 2 ? 8 : 0);
-        const int n = n0 + wn + j * 8 + tig * 2 + (e & 1);
-        if (m >= g.M || n >= g.N) continue;
-        float v = acc[i][j][e] * g.alpha;
+      for (int j = 0; j < 16; ++j) {
+        const int n = n0 + c0 + j;
+        if (n >= g.N) break;
+        float v = __uint_as_float(r[j]) * g.alpha;
         if (g.bias) v += g.bias[n];
         if (g.relu) v = fmaxf(v, 0.f);
         if (g.mask) v *= (float)g.mask[(size_t)m * g.N + n];
@@ -107,6 +174,13 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(GemmArgs g) {
         if (g.C) g.C[(size_t)m * g.ldc + n] = v;
         if (g.Cb) g.Cb[(size_t)m * g.ldc + n] = __float2bfloat16(v);
       }
+    }
+  } else if (threadIdx.x == 0) {
+    atomicExch(&g_tc_timeout, 1);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, TBN);
 }
 
 // dz = sigmoid(z) - target; loss partials: softplus(z) - target * z (per block, float64).
@@ -200,9 +274,27 @@ __global__ void logq_kernel(const float* __restrict__ z, const __nv_bfloat16* __
 
 int gemm_bf16(const GemmArgs& g, cudaStream_t s) {
   if (g.M <= 0 || g.N <= 0 || g.K <= 0 || !g.A || !g.B || (!g.C && !g.Cb)) return fail(RGS_ERR_ARG, "bad GEMM");
-  dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM);
-  gemm_bf16_kernel<<<grid, 128, 0, s>>>(g);
+  static bool configured[64] = {false};
+  int device = 0;
+  RGS_CUDA_TRY(cudaGetDevice(&device));
+  if (device >= 0 && device < 64 && !configured[device]) {
+    RGS_CUDA_TRY(cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem));
+    configured[device] = true;
+  }
+  dim3 grid((g.N + TBN - 1) / TBN, (g.M + TBM - 1) / TBM);
+  gemm_tc_kernel<<<grid, 128, kGemmSmem, s>>>(g);
   RGS_CUDA_TRY(cudaGetLastError());
+  return RGS_OK;
+}
+
+int tensor_core_status(int* timed_out) {
+  int h = 0, zero = 0;
+  RGS_CUDA_TRY(cudaMemcpyFromSymbol(&h, g_tc_timeout, sizeof(int)));
+  RGS_CUDA_TRY(cudaMemcpyToSymbol(g_tc_timeout, &zero, sizeof(int)));
+  int w = 0;
+  int rc = wht_tensor_core_timeout(&w);
+  if (rc) return rc;
+  *timed_out = h | w;
   return RGS_OK;
 }
 

@@ -22,6 +22,8 @@ struct GemmArgs {
 };
 
 int gemm_bf16(const GemmArgs& g, cudaStream_t s);
+// Reads and clears the flag that a bounded tensor-core wait gave up (synchronous).
+int tensor_core_status(int* timed_out);
 int bce_grad(const float* z, const float* target, int count, float scale, __nv_bfloat16* dz, double* partial,
              int blocks, cudaStream_t s);
 int colsum_bf16(const __nv_bfloat16* x, int rows, int cols, float* out, cudaStream_t s);

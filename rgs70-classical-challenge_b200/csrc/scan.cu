@@ -385,7 +385,7 @@ cudaError_t launch_pair(int precision, int Bt, int device, cudaStream_t s, const
   const int lS = lC - lL;
   if (lS > 3) return cudaErrorInvalidValue;  // more column slices than warps in a block
   const int loads = pair_nc(P.codeA) * pair_nc(P.codeB);
-  const int U = loads >= 8 ? 1 : 8 / loads;
+  const int U = loads >= RGS_PAIR_LOADS ? 1 : RGS_PAIR_LOADS / loads;
   const unsigned long long groups = 1ull << (P.m - P.dw);
   const unsigned long long per_warp = (unsigned long long)U << (5 - lL);
   const unsigned long long warps = ((groups + per_warp - 1) / per_warp) << lS;

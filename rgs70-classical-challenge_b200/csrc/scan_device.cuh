@@ -11,6 +11,15 @@
 
 #include "plan.hpp"
 
+// Launch shape of the fused pair kernel (scan_pair.cuh): resident 256-thread blocks per
+// SM (two: 128 registers per thread) and gathers in flight per lane and loop iteration.
+#ifndef RGS_PAIR_MINB
+#define RGS_PAIR_MINB 2
+#endif
+#ifndef RGS_PAIR_LOADS
+#define RGS_PAIR_LOADS 8
+#endif
+
 namespace rgs {
 
 typedef unsigned long long u64;

@@ -1,21 +1,27 @@
 // Allocation-free variant of the batched scan executor.
 //
-// Some callers cannot allocate device memory at call time: code running inside a
-// host callback or a signal-safe section, hosts that hand this library a fixed
-// device-memory budget and forbid it from growing, or integrations whose own
-// allocator owns every byte and would not see a cudaMalloc made behind its back.
-// rgs_scan_amplitudes_noalloc serves them: the caller passes only inputs and outputs,
-// and all scratch (the plan tables, the two ping-pong environment tables, per-item
-// weights and per-step maxima) lives in one file-scope device array of fixed size,
-// RGS_NOALLOC_SCRATCH_BYTES, which every GPU that loads this library holds until
-// the process exits.
+// Some callers cannot let this library allocate device memory: hosts that hand it a
+// fixed device-memory budget and forbid it from growing, and integrations whose own
+// allocator owns every byte of the GPU and would not see a cudaMalloc made behind its
+// back.  rgs_scan_amplitudes_noalloc serves them: the caller passes only inputs and
+// outputs, and all scratch (the step byte tables, the two ping-pong environment
+// tables, per-item weights and per-step maxima) lives in one file-scope device array
+// of fixed size, RGS_NOALLOC_SCRATCH_BYTES, which every GPU that loads this library
+// holds until the process exits.  "Allocation-free" means no device allocation only:
+// the call still takes a host mutex, builds small host vectors, makes CUDA runtime
+// calls and launches kernels, so it must not be called from a CUDA host callback
+// (cudaLaunchHostFunc / stream callbacks forbid CUDA calls) or from a signal handler.
 //
 // Set-up: the first call on a device, with that device current, looks up the
-// device address of the array with cudaGetSymbolAddress and caches it; that first
-// call should come before any stream capture.  The array is shared by every call
-// and keeps the last call's contents; everything that must start at zero is
-// cleared by the call itself.  Calls whose work overlaps on the GPU (different
-// streams, or threads without ordering) race on the array: serialise them.
+// device address of the array with cudaGetSymbolAddress and caches it for the life
+// of the process; a cudaDeviceReset on that device invalidates the cached address,
+// so the library must not be used on a device after it was reset.  Every call
+// uploads the plan's step tables and vertex records from host memory with pageable
+// copies, so it is rejected (RGS_ERR_UNSUPPORTED) on a stream that is being captured.
+// The array is shared by every call and keeps the last call's contents; everything
+// that must start at zero is cleared by the call itself.  Calls whose work overlaps
+// on the GPU (different streams, or threads without ordering) race on the array:
+// serialise them.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -54,11 +60,19 @@ struct NoallocLayout {
   ScanLayout ws;
 };
 
+// u64 entries of the per-step byte tables: they come first in plan.tables, before the
+// tables of fused pairs, which the position-by-position sweep here never reads.
+size_t step_table_entries(const Plan& plan) {
+  size_t n = 0;
+  for (const auto& d : plan.dev) n = std::max(n, (size_t)d.table_off + ((size_t)d.nbytes << 8));
+  return n;
+}
+
 int noalloc_layout(const Plan& plan, int Bt, int precision, NoallocLayout& L) {
   int rc = scan_layout(plan, Bt, precision, L.ws);
   if (rc) return rc;
   L.off_tables = 0;
-  L.off_verts = align_up(std::max<size_t>(1, plan.tables.size()) * sizeof(unsigned long long), 256);
+  L.off_verts = align_up(std::max<size_t>(1, step_table_entries(plan)) * sizeof(unsigned long long), 256);
   L.off_ws = L.off_verts + align_up(sizeof(DevVert) * plan.n, 256);
   L.total = L.off_ws + L.ws.total();
   return RGS_OK;
@@ -79,6 +93,11 @@ extern "C" int rgs_scan_amplitudes_noalloc(rgs_plan* handle, const double* unita
   Plan& plan = handle->plan;
   if (!plan.exec_ok) return fail(RGS_ERR_UNSUPPORTED, plan.exec_reason);
   cudaStream_t stream = (cudaStream_t)stream_ptr;
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  RGS_CUDA_TRY(cudaStreamIsCapturing(stream, &capture));
+  if (capture != cudaStreamCaptureStatusNone)
+    return fail(RGS_ERR_UNSUPPORTED, "rgs_scan_amplitudes_noalloc uploads plan data from pageable host memory on "
+                                     "every call: call it on a stream that is not being captured");
 
   // Largest batch tile (<= 64 items) whose layout fits the fixed scratch array.
   NoallocLayout L;
@@ -104,7 +123,7 @@ extern "C" int rgs_scan_amplitudes_noalloc(rgs_plan* handle, const double* unita
   if (rc) return rc;
   char* scratch = (char*)base;
 
-  // Plan tables and vertex records into the scratch (copies, not allocations).
+  // Step tables and vertex records into the scratch (copies, not allocations).
   std::vector<DevVert> verts(plan.n);
   for (int j = 0; j < plan.n; ++j) {
     verts[j].fut_lo = (unsigned long long)plan.future[j];
@@ -114,8 +133,9 @@ extern "C" int rgs_scan_amplitudes_noalloc(rgs_plan* handle, const double* unita
   }
   unsigned long long* tables = (unsigned long long*)(scratch + L.off_tables);
   DevVert* d_verts = (DevVert*)(scratch + L.off_verts);
-  if (!plan.tables.empty())
-    RGS_CUDA_TRY(cudaMemcpyAsync(tables, plan.tables.data(), plan.tables.size() * sizeof(unsigned long long),
+  const size_t ntab = step_table_entries(plan);
+  if (ntab)
+    RGS_CUDA_TRY(cudaMemcpyAsync(tables, plan.tables.data(), ntab * sizeof(unsigned long long),
                                  cudaMemcpyHostToDevice, stream));
   RGS_CUDA_TRY(cudaMemcpyAsync(d_verts, verts.data(), sizeof(DevVert) * plan.n, cudaMemcpyHostToDevice, stream));
 

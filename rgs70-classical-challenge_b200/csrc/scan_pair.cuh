@@ -31,8 +31,9 @@ struct PairMode {
   static constexpr int ng0 = C == PC_P1 ? 1 : (C == PC_P2H ? 1 : (C == PC_P2F ? 2 : (C == PC_P4H ? 2 : 2)));
 };
 
-// Group index arithmetic in the index type I: 32-bit where every rank of the pair is at
-// most 31 (fewer instructions per group), 64-bit otherwise.
+// Group index and chunk offset arithmetic in the index type I: 32-bit where every rank
+// of the pair plus log2(chunks per row) is at most 31 (fewer instructions per group),
+// 64-bit otherwise.
 template <typename I>
 __device__ __forceinline__ int parity_of(I x);
 template <>
@@ -68,11 +69,11 @@ __device__ __forceinline__ I deposit_pivots(I it, const DevPair& P) {
   return q;
 }
 
-// Two 256-thread blocks per SM (128 registers) where the registers suffice; one for
-// float64 arithmetic on complex64 tables, whose conversions need more.
+// Resident 256-thread blocks per SM: RGS_PAIR_MINB (scan_device.cuh) where the registers
+// suffice; one for float64 arithmetic on complex64 tables, whose conversions need more.
 template <typename S, typename M>
 struct PairBlocks {
-  static constexpr int value = sizeof(M) > sizeof(S) ? 1 : 2;
+  static constexpr int value = sizeof(M) > sizeof(S) ? 1 : RGS_PAIR_MINB;
 };
 
 template <typename S, typename M, int VE, int CA, int CB, typename I>
@@ -88,8 +89,11 @@ __global__ void __launch_bounds__(256, PairBlocks<S, M>::value)
   constexpr int NUA = NCB;                      // A units: register pairs (PAIR A) or registers
   constexpr int NUB = MA::pair ? 2 : 1;         // B units
   constexpr int LOADS = NUA * NCA;
-  constexpr int U = LOADS >= 8 ? 1 : 8 / LOADS;  // groups per lane per iteration
+  constexpr int U = LOADS >= RGS_PAIR_LOADS ? 1 : RGS_PAIR_LOADS / LOADS;  // groups per lane per iteration
   __shared__ u64 smax[256];
+  // Group maps of the low bits of a group index (see the loop below), per block.
+  __shared__ I s_low[256][2];
+  __shared__ unsigned char s_lowpar[256];
   const int Bt = 1 << lbt;
   const int lC = lbt - (VE == 2 ? 1 : 0);  // log2 chunks per row
   const int lL = lC < 5 ? lC : 5;          // log2 lanes per row
@@ -149,21 +153,36 @@ __global__ void __launch_bounds__(256, PairBlocks<S, M>::value)
   S mx[VE];
 #pragma unroll
   for (int v = 0; v < VE; ++v) mx[v] = (S)0;
+  // A warp iteration takes the groups base | idx, idx < per_iter (base a multiple of
+  // per_iter).  q0 (zeros deposited at W's pivots), both table maps and the parity of
+  // q0 & beta_B are GF(2)-linear in the group index, so the part of idx comes from this
+  // block table and only base needs the byte-table lookups, once per iteration.
+  for (int i = threadIdx.x; i < (int)per_iter; i += blockDim.x) {
+    const I q = deposit_pivots<I>((I)i, P);
+    I pl = 0, cl = 0;
+    lookup2_as<I>(T2, P.nbMB, q, pl, cl);
+    s_low[i][0] = pl;
+    s_low[i][1] = cl;
+    s_lowpar[i] = (unsigned char)parity_of<I>(q & betaB);
+  }
+  __syncthreads();
 
   for (u64 base = (gwarp >> lS) * per_iter; base < groups; base += wslice * per_iter) {
     bool ok[U];
     I c0[U];
     int pq[U], ya[U][NUA], pa[U][NUA][NCA];
     Chunk<S, VE> e[U][NUA][NCA];
+    const I qb = deposit_pivots<I>((I)base, P);
+    I pb = 0, cb = 0;
+    lookup2_as<I>(T2, P.nbMB, qb, pb, cb);
+    const int pqb = parity_of<I>(qb & betaB);
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      const u64 it = base + ((u64)u << lR) + sub;
-      ok[u] = it < groups;
-      const I q0 = ok[u] ? deposit_pivots<I>((I)it, P) : (I)0;
-      I p0 = 0, cq = 0;
-      if (ok[u]) lookup2_as<I>(T2, P.nbMB, q0, p0, cq);
-      c0[u] = cq;
-      pq[u] = parity_of<I>(q0 & betaB);
+      const int idx = (u << lR) + sub;
+      ok[u] = base + (u64)idx < groups;
+      const I p0 = pb ^ s_low[idx][0];
+      c0[u] = cb ^ s_low[idx][1];
+      pq[u] = pqb ^ (int)s_lowpar[idx];
 #pragma unroll
       for (int a = 0; a < NUA; ++a) {
         const I pu = p0 ^ (I)P.LAw[a];
@@ -172,7 +191,7 @@ __global__ void __launch_bounds__(256, PairBlocks<S, M>::value)
         for (int k = 0; k < NCA; ++k) {
           const I row = (pu ^ (I)P.combA[k]) & maskA;
           pa[u][a][k] = parity_of<I>(row & betaA);
-          if (ok[u]) e[u][a][k].load(Ein, ((u64)row << lC) + col);
+          if (ok[u]) e[u][a][k].load(Ein, (u64)(((I)row << lC) | (I)col));
         }
       }
     }
@@ -250,8 +269,8 @@ __global__ void __launch_bounds__(256, PairBlocks<S, M>::value)
 #pragma unroll
       for (int b = 0; b < NUB; ++b) {
         const I cx = c0[u] ^ (I)P.MB0[b];
-        outX[b].store(Eout, ((u64)cx << lC) + col);
-        if (MB::pair) outY[b].store(Eout, ((u64)(cx ^ (I)P.tB) << lC) + col);
+        outX[b].store(Eout, (u64)(((I)cx << lC) | (I)col));
+        if (MB::pair) outY[b].store(Eout, (u64)(((I)(cx ^ (I)P.tB) << lC) | (I)col));
       }
     }
   }

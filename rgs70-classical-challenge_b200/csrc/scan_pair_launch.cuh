@@ -44,13 +44,15 @@ cudaError_t launch_pair_a(dim3 grid, cudaStream_t s, const void* Ein, void* Eout
 #undef RGS_PAIR_A
 }
 
-// 32-bit group index arithmetic when the pair's input (with its y bit), intermediate and
-// output ranks all fit in 31 bits.
+// 32-bit group index and chunk offset arithmetic when the pair's input (with its y bit),
+// intermediate and output ranks fit in 31 bits, and so do the chunk offsets of the input
+// and output rows (rank + log2 chunks per row).
 template <typename S, typename M, int VE>
 cudaError_t launch_pair_codes(dim3 grid, cudaStream_t s, const void* Ein, void* Eout, const DevPair& P,
                               const u64* tables, const double4* WA, const double4* WB, const u64* mp, u64* mA,
                               u64* mc, int lbt, u64 es) {
-  if (P.a <= 30 && P.m <= 31 && P.o <= 31)
+  const int lC = lbt - (VE == 2 ? 1 : 0);
+  if (P.a <= 30 && P.m <= 31 && P.o <= 31 && P.a + lC <= 31 && P.o + lC <= 31)
     return launch_pair_a<S, M, VE, unsigned>(grid, s, Ein, Eout, P, tables, WA, WB, mp, mA, mc, lbt, es);
   return launch_pair_a<S, M, VE, u64>(grid, s, Ein, Eout, P, tables, WA, WB, mp, mA, mc, lbt, es);
 }

@@ -239,13 +239,23 @@ def _state(state):
     return state
 
 
-def fwht(state, lo=0, hi=None):
-    """In-place Walsh-Hadamard butterflies on bits [lo, hi) of a complex64 CUDA tensor."""
+WHT_PRECISIONS = {"fp32": 0, "split_bf16x2": 2, "split_bf16x3": 3}
+
+
+def fwht(state, lo=0, hi=None, precision="fp32"):
+    """In-place Walsh-Hadamard butterflies (x + y, x - y) on bits [lo, hi) of a complex64
+    CUDA tensor.  ``precision``: "fp32" (FP32 butterflies), or 16 x 16 Hadamard blocks on the
+    tensor cores over a split-BF16 copy of every value, "split_bf16x2" (two BF16 terms,
+    about 4e-6 relative error per 4-bit round) or "split_bf16x3" (three terms, FP32 level);
+    the tensor-core variants need at least 2^12 values."""
     _state(state)
+    if precision not in WHT_PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(WHT_PRECISIONS)}")
     nbits = int(state.numel()).bit_length() - 1
     hi = nbits if hi is None else hi
     with torch.cuda.device(state.device):
-        _lib.check(_lib.lib().rgs_fwht(ctypes.c_void_p(state.data_ptr()), nbits, lo, hi, _stream(state.device)))
+        _lib.check(_lib.lib().rgs_fwht_precision(ctypes.c_void_p(state.data_ptr()), nbits, lo, hi,
+                                                 WHT_PRECISIONS[precision], _stream(state.device)))
 
 
 def product(state, unitaries, lo=0, hi=None):

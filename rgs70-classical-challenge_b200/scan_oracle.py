@@ -305,4 +305,30 @@ class ScanOracle:
         return amp
 
     def probabilities(self, bits):
+        """p(x) in this oracle's precision.  Complex64 results carry the storage rounding
+        of the tables, which is relative to each table's maximum, not to the amplitude:
+        for p(x) >= 0.01 * 2^-n the relative error stays below 1e-4, for smaller p it can
+        exceed it; ``checked_probabilities`` states the error of every result."""
         return np.abs(self.amplitudes(bits)) ** 2
+
+    def checked_probabilities(self, bits, tol=1e-4):
+        """p(x) with its error against FP64 stated per result.
+
+        Runs this oracle's precision (the bulk) and the complex128 scan (the recheck) on
+        the same strings.  Returns ``(p, rel_err, fp64_used)``: ``rel_err[i]`` =
+        |p_bulk - p_fp64| / p_fp64 of result i; ``p[i]`` is the bulk value where
+        ``rel_err[i] <= tol`` and the FP64 value elsewhere (``fp64_used[i]`` True), so
+        every returned probability is within ``tol`` of the FP64 scan."""
+        p_bulk = self.probabilities(bits)
+        if self.engine.precision == "c128":
+            return p_bulk, np.zeros_like(p_bulk), np.zeros(len(p_bulk), dtype=bool)
+        if getattr(self, "_fp64", None) is None:
+            self._fp64 = ScanEngine(self.plan, self.u, device=self.engine.device, precision="c128")
+        val, ls = self._fp64.sweep_bits(bits)
+        p64 = np.abs(amplitudes_from(val, ls, self.n)) ** 2
+        if not np.all(np.isfinite(p64)):
+            raise ArithmeticError("non-finite probability from the complex128 recheck")
+        with np.errstate(divide="ignore", invalid="ignore"):
+            rel = np.where(p64 > 0, np.abs(p_bulk - p64) / p64, np.where(p_bulk == 0, 0.0, np.inf))
+        use = rel > tol
+        return np.where(use, p64, p_bulk), rel, use

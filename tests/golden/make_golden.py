@@ -1,7 +1,8 @@
 """Generate the golden fixtures in this directory by running the REFERENCE code.
 
-Imports whyihaveyou/rgs70-classical-challenge read-only from /root/reference
-(or the path in RGS_REFERENCE) -- it never writes there -- and stores small
+Imports whyihaveyou/rgs70-classical-challenge read-only from the checkout named by
+``--reference PATH`` or the RGS_REFERENCE environment variable (there is no default)
+-- it never writes there -- and stores small
 input/output vectors that pin the CPU oracle (``oracle/``) and the CUDA engine:
 
 * ``plans.json``        reference ``make_plan`` / ``future_masks`` output for
@@ -20,7 +21,8 @@ input/output vectors that pin the CPU oracle (``oracle/``) and the CUDA engine:
                         Born samples of RGS70 (born/batch{1,2}/*_fp64.jsonl), the
                         empirical law of p(x) under Born sampling.
 
-Run from the repository root:  python tests/golden/make_golden.py [born]
+Run from the repository root:
+    python tests/golden/make_golden.py --reference PATH [born]
 (``born`` rewrites only rgs70_born.json).
 """
 import importlib.util
@@ -32,7 +34,19 @@ from pathlib import Path
 import numpy as np
 
 sys.dont_write_bytecode = True
-REF = Path(os.environ.get("RGS_REFERENCE", "/root/reference"))
+
+def _reference_root(argv):
+    """The reference checkout: ``--reference PATH`` or $RGS_REFERENCE, else exit."""
+    if "--reference" in argv:
+        k = argv.index("--reference")
+        if k + 1 < len(argv):
+            return Path(argv[k + 1]), argv[:k] + argv[k + 2:]
+    if os.environ.get("RGS_REFERENCE"):
+        return Path(os.environ["RGS_REFERENCE"]), argv
+    sys.exit("make_golden.py: name the reference checkout with --reference PATH or RGS_REFERENCE")
+
+
+REF, ARGS = (_reference_root(sys.argv[1:]) if __name__ == "__main__" else (Path("."), []))
 W = REF / "work" / "rgs_attack"
 OUT = Path(__file__).resolve().parent
 
@@ -107,7 +121,7 @@ def born_records():
 
 
 def main():
-    if sys.argv[1:] == ["born"]:
+    if ARGS == ["born"]:
         born_records()
         return
     born_records()

@@ -208,3 +208,35 @@ def test_index_map_and_phase(pkg, fixtures):
     assert np.abs(dst.cpu().numpy() - ref).max() < 1e-6 * np.abs(ref).max()
     pkg._lib.check(lib.rgs_fourier_quadphase(s._h, ctypes.c_void_p(src.data_ptr()), stream))
     assert np.array_equal(src.cpu().numpy(), (x * phase).astype(np.complex64))
+
+
+@pytest.mark.parametrize("nbits,lo,hi", [(12, 0, 12), (14, 1, 13), (17, 0, 17), (21, 3, 20), (22, 0, 22)])
+def test_tensor_core_wht_precision(pkg, nbits, lo, hi):
+    """16 x 16 Hadamard blocks on the tensor cores (tcgen05) over split-BF16 values
+    against the FP64 oracle: relative L2 error <= 3e-5 with two BF16 terms, <= 1e-6 with
+    three (FP32 butterflies: <= 1e-6); the GEMM flag of a bounded wait stays clear."""
+    import ctypes
+    rng = np.random.default_rng(nbits + lo)
+    x = (rng.standard_normal(1 << nbits) + 1j * rng.standard_normal(1 << nbits)).astype(np.complex64)
+    ref = x.astype(np.complex128)
+    for q in range(lo, hi):  # butterfly (x + y, x - y) on bit q of the flat index, as gs.apply_one
+        v = ref.reshape(-1, 2, 1 << q)
+        ref = np.stack([v[:, 0] + v[:, 1], v[:, 0] - v[:, 1]], axis=1).reshape(-1)
+    errs = {}
+    for prec in ("fp32", "split_bf16x2", "split_bf16x3"):
+        d = torch.from_numpy(x.copy()).cuda()
+        pkg.fwht(d, lo, hi, precision=prec)
+        got = d.cpu().numpy().astype(np.complex128)
+        errs[prec] = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+    assert errs["fp32"] < 1e-6, errs
+    assert errs["split_bf16x3"] < 1e-6, errs
+    assert errs["split_bf16x2"] < 3e-5, errs
+    flag = ctypes.c_int32(-1)
+    pkg._lib.check(pkg._lib.lib().rgs_tensor_core_status(ctypes.byref(flag)))
+    assert flag.value == 0
+
+
+def test_tensor_core_wht_rejects_small_states(pkg):
+    d = torch.zeros(1 << 10, dtype=torch.complex64, device="cuda")
+    with pytest.raises(NotImplementedError):
+        pkg.fwht(d, precision="split_bf16x3")

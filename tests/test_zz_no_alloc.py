@@ -1,9 +1,9 @@
 """The allocation-free scan entry point agrees with the allocating one.
 
-rgs_scan_amplitudes_noalloc exists for callers that cannot allocate device memory
-when they call in (host callbacks, hosts that fix the library's memory budget,
-integrations whose allocator must own every byte): it takes only inputs and
-outputs and keeps its scratch in a static device array.  This file is collected
+rgs_scan_amplitudes_noalloc exists for callers that cannot let the library allocate
+device memory (hosts that fix the library's memory budget, integrations whose
+allocator must own every byte of the GPU): it takes only inputs and outputs and
+keeps its scratch in a static device array.  This file is collected
 last so a failure here does not hide the rest of the suite.  Each test calls the
 new entry point through the C ABI twice in a row (different batches, so stale
 scratch from the first call would show) and compares with rgs_scan_amplitudes.
@@ -48,6 +48,41 @@ def test_noalloc_matches_workspace_entry_point(pkg, precision, tol):
         ref = pkg.amplitudes_from(ref_v, ref_l, inst.n)
         rel = np.abs(np.abs(got) ** 2 - np.abs(ref) ** 2) / np.abs(ref) ** 2
         assert rel.max() < tol
+
+
+def test_noalloc_fixed_vertices(pkg):
+    """A plan with structurally fixed vertices: the per-item flag bytes and affine
+    offsets live in the shared scratch too (diagonal / anti-diagonal gates)."""
+    import torch
+    from oracle import scan_plan as sp
+
+    rng = np.random.default_rng(41)
+    n = 20
+    g = pkg.instances.regular3(n, rng)
+    u = pkg.instances.haar_su2(n, rng)
+    for k, q in enumerate(rng.choice(n, size=6, replace=False)):
+        ph = np.exp(1j * rng.uniform(0, 2 * np.pi, 2))
+        u[q] = np.diag(ph) if k % 2 == 0 else np.array([[0, ph[0]], [ph[1], 0]])
+    fixed = sp.structurally_fixed(u, n)
+    assert len(fixed) == 6
+    plan = pkg.ScanPlan(n, pkg.edges_from_graph(g), rng.permutation(n).tolist(), fixed)
+    for precision, tol in (("c64", 1e-4), ("c128", 1e-12)):
+        eng = pkg.ScanEngine(plan, u, precision=precision)
+        vdt = torch.complex128 if precision == "c128" else torch.complex64
+        for batch, seed in ((129, 5), (64, 6)):
+            bits = pkg.instances.uniform_bits(batch, n, np.random.default_rng(seed))
+            ref = pkg.amplitudes_from(*eng.sweep_bits(bits), n)
+            d_bits = torch.from_numpy(pkg.pack_bits(bits, n).view(np.int64)).cuda()
+            out_v = torch.empty(batch, dtype=vdt, device="cuda")
+            out_l = torch.empty(batch, dtype=torch.float64, device="cuda")
+            pkg._lib.check(_noalloc(pkg, plan, eng.d_u, d_bits, batch, pkg.PRECISIONS[precision], out_v, out_l))
+            torch.cuda.synchronize()
+            got = pkg.amplitudes_from(out_v.cpu().numpy(), out_l.cpu().numpy(), n)
+            nz = np.abs(ref) > 1e-12
+            assert nz.any()
+            assert np.all(np.abs(got[~nz]) < 1e-12)
+            rel = np.abs(np.abs(got[nz]) ** 2 - np.abs(ref[nz]) ** 2) / np.abs(ref[nz]) ** 2
+            assert rel.max() < tol
 
 
 def test_noalloc_rejects_plans_beyond_its_scratch(pkg):
