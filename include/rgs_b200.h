@@ -262,6 +262,21 @@ int rgs_fourier_masses(rgs_fourier* plan, const void* state, void* workspace, do
  * Fails with RGS_ERR_ZERO_NORM when |norm - 1| > 1e-3 (distributed_sampler.py:151). */
 int rgs_fourier_draw(rgs_fourier* plan, const void* state, void* workspace, double u1, double u2, double u3,
                      uint64_t* index, double* pa, double* norm, void* stream);
+/* Two-shard conditional state (the top bit m - 1 split over two devices, one shard per
+ * device; DeferredGlobalMixin, deferred_global_sampler.py:40-88, with the initcov_global
+ * fold of the top bit's Walsh factor, :23-37).  rgs_fourier_compute_shard: this device's
+ * half (top bit == shard) in `state` (complex64[2^(m-1)]), deferred terminal unitary not
+ * applied, its tile masses in the workspace; needs deferred != 0 and m >= 13.  No data
+ * crosses devices.  rgs_fourier_shard_mass: total mass of the computed shard
+ * (synchronises).  rgs_fourier_shard_draw: two-level inverse CDF inside the shard (u1:
+ * tile, u2: element), the local index (synchronises).  The draw across shards (which
+ * shard, then the terminal pair U_last (v_0[l], v_1[l]) with u3) exchanges two scalars per
+ * shard: see ShardedConditionalSampler. */
+int rgs_fourier_compute_shard(rgs_fourier* plan, uint64_t outB, int32_t shard, void* state, void* workspace,
+                              size_t workspace_bytes, void* stream);
+int rgs_fourier_shard_mass(rgs_fourier* plan, void* workspace, double* mass, void* stream);
+int rgs_fourier_shard_draw(rgs_fourier* plan, const void* state, void* workspace, double u1, double u2,
+                           uint64_t* local_index, void* stream);
 /* Index map with q_A phase (permute, distributed_sampler.py:35-41), dst != src. */
 int rgs_fourier_index_map(rgs_fourier* plan, const void* src, void* dst, void* stream);
 /* state[z] *= (-1)^{q_A(z)} (quadratic_phase, graph_sampler.py:76-85). */

@@ -223,6 +223,33 @@ def cpu_deferred(g, u, A, B, outB):
     return raw, final
 
 
+def cpu_shards(g, u, A, B, outB):
+    """The two halves (top A bit = shard) of the state before the terminal unitary, each
+    computed with shard-local operations only: the reference's two-device split
+    (``np.split`` emulation of ``fourier_fused_sampler.py:161-169``) with the top bit's Walsh
+    factor folded into the initialisation (``initcov_global``,
+    ``deferred_global_sampler.py:23-37``); the q_A phase uses the global index."""
+    g = np.asarray(g)
+    m = len(A)
+    N = gf2_inverse(g[np.ix_(B, A)]).T
+    ids = np.arange(1 << (m - 1), dtype=np.uint64)
+    inits = []
+    for bit in (0, 1):
+        b = map_indices(ids | (np.uint64(bit) << np.uint64(m - 1)), N)
+        v = np.full(len(ids), 2.0 ** (-m / 2), dtype=np.complex128)
+        for j, site in enumerate(B):
+            v *= np.asarray(u[site])[outB[j], ((b >> np.uint64(j)) & np.uint64(1)).astype(np.int64)]
+        v *= phase_for_ids(b, g[np.ix_(B, B)])
+        inits.append(v)
+    shards = [inits[0] + inits[1], inits[0] - inits[1]]
+    for s, v in enumerate(shards):
+        walsh(v)
+        v *= phase_for_ids(ids | (np.uint64(s) << np.uint64(m - 1)), g[np.ix_(A, A)])
+        for j, site in enumerate(A[:-1]):
+            apply_one(v, np.asarray(u[site]), j)
+    return shards
+
+
 # ----------------------------------------------------------------------------- LUT specialisation
 def transformed_quadratic(graph_B, N):
     """q(N z) = sum_{i<j} Q_ij z_i z_j + ell . z over GF(2) (``init_specialization.py:53-59``)."""

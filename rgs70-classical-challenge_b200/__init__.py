@@ -11,7 +11,7 @@ from .plan import ScanPlan, Step, make_plan, future_masks, rank_profile, byte_ta
 from .scan_oracle import ScanEngine, ScanOracle, pack_bits, amplitudes_from, PRECISIONS, capture_graph, autotune_tile, \
     max_batch_tile
 from . import instances
-from .samplers import ConditionalSampler, DrawRecorder, produce, fwht, product, block_mass
+from .samplers import ConditionalSampler, ShardedConditionalSampler, DrawRecorder, produce, fwht, product, block_mass
 from .chain import ChainSampler, unpack_bits
 from .batch import ResidentBatch
 from . import batch
@@ -23,6 +23,6 @@ from .proposal import MadeProposal, rejection_sample, capped_rejection, calibrat
 __all__ = [
     "ScanPlan", "Step", "make_plan", "future_masks", "rank_profile", "byte_tables", "kernel_combos",
     "edges_from_graph", "search_order", "ScanEngine", "ScanOracle", "pack_bits", "amplitudes_from", "PRECISIONS", "capture_graph", "autotune_tile",
-    "ConditionalSampler", "DrawRecorder", "produce", "fwht", "product", "block_mass", "ChainSampler", "unpack_bits", "ResidentBatch",
+    "ConditionalSampler", "ShardedConditionalSampler", "DrawRecorder", "produce", "fwht", "product", "block_mass", "ChainSampler", "unpack_bits", "ResidentBatch",
     "MadeProposal", "rejection_sample", "capped_rejection", "calibrate_envelope",
 ]

@@ -117,6 +117,11 @@ SIGNATURES = {
     "rgs_fourier_create": (ctypes.c_int, [ctypes.c_int32, c_uint8_p, c_double_p, ctypes.c_int32, c_int32_p,
                                           c_int32_p, ctypes.c_int32, ctypes.POINTER(c_void_p)]),
     "rgs_fourier_destroy": (None, [c_void_p]),
+    "rgs_fourier_compute_shard": (ctypes.c_int, [c_void_p, ctypes.c_uint64, ctypes.c_int32, c_void_p, c_void_p,
+                                                 ctypes.c_size_t, c_void_p]),
+    "rgs_fourier_shard_mass": (ctypes.c_int, [c_void_p, c_void_p, c_double_p, c_void_p]),
+    "rgs_fourier_shard_draw": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_double, ctypes.c_double,
+                                              ctypes.POINTER(ctypes.c_uint64), c_void_p]),
     "rgs_fourier_info": (ctypes.c_int, [c_void_p, c_int32_p, c_int32_p, c_int32_p, ctypes.POINTER(ctypes.c_int64),
                                         c_int32_p]),
     "rgs_fourier_tables": (ctypes.c_int, [c_void_p, c_uint64_p, c_uint64_p, c_uint64_p, c_uint64_p, c_int32_p]),

@@ -73,6 +73,24 @@ int rgs_fourier_workspace_bytes(const rgs_fourier* f, size_t* bytes) {
   return RGS_OK;
 }
 
+int rgs_fourier_compute_shard(rgs_fourier* f, uint64_t outB, int32_t shard, void* state, void* workspace,
+                              size_t workspace_bytes, void* stream) {
+  if (!f) return fail(RGS_ERR_ARG, "plan is NULL");
+  if (f->plan.m < 64 && (outB >> f->plan.m) != 0) return fail(RGS_ERR_ARG, "outB has bits above m");
+  return fourier_compute_shard(f->plan, outB, shard, state, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int rgs_fourier_shard_mass(rgs_fourier* f, void* workspace, double* mass, void* stream) {
+  if (!f) return fail(RGS_ERR_ARG, "plan is NULL");
+  return fourier_shard_mass(f->plan, workspace, mass, (cudaStream_t)stream);
+}
+
+int rgs_fourier_shard_draw(rgs_fourier* f, const void* state, void* workspace, double u1, double u2,
+                           uint64_t* local_index, void* stream) {
+  if (!f) return fail(RGS_ERR_ARG, "plan is NULL");
+  return fourier_shard_draw(f->plan, state, workspace, u1, u2, local_index, (cudaStream_t)stream);
+}
+
 int rgs_fourier_tune(rgs_fourier* f, void* state, void* workspace, size_t workspace_bytes, void* stream,
                      int32_t* variant, float* ms) {
   if (!f) return fail(RGS_ERR_ARG, "plan is NULL");

@@ -46,7 +46,7 @@ FourierPlan::~FourierPlan() {
   cudaGetDevice(&prev);
   cudaSetDevice(device);
   for (void* p : {d_lut_z, d_lut_a, d_lut_cols, d_uA, d_uB, d_rot, d_dg, d_dh, d_rg, d_rh, d_tt_init, d_tt_phase,
-                  d_qsym_z, d_qsym_a})
+                  d_tt_init_shard, d_tt_phase_shard, d_qsym_z, d_qsym_a})
     if (p) cudaFree(p);
   if (prev >= 0) cudaSetDevice(prev);
 }
@@ -87,6 +87,13 @@ struct PassParams {
   int variant;                    // launch variant (see fourier_pass_kernel)
   double* masses;                 // per tile or null
   int store;
+  // Sharded state (top bit of the index split over devices): v holds the global indices
+  // g with g & ~amask fixed, at v[g & amask]; a launch runs tiles [tile0, tile0 + grid);
+  // store_top >= 0 stores only the elements whose top bit (m - 1) equals it.
+  u64 amask;
+  u64 tile0;
+  u64 ntiles;                     // tiles of this launch (0: every tile of the index space)
+  int store_top;
 };
 
 // Padded shared-memory layout: one spare slot per 16 elements, so the 16 threads of a
@@ -342,7 +349,7 @@ __global__ void __launch_bounds__(256, MINB) fourier_pass_kernel(const __grid_co
   __shared__ unsigned s_lm;
   const int TB = P.c + P.K;
   const int nt = 1 << (TB - 4);
-  const u64 tile = blockIdx.x;
+  const u64 tile = blockIdx.x + P.tile0;
   const u64 base = tile_global(P, tile, 0);
   const u64 varying = ((1ull << P.c) - 1ull) | (((1ull << P.K) - 1ull) << P.q);
   // Load (or compute) the tile: each thread owns 8 element pairs (16-byte accesses,
@@ -383,7 +390,7 @@ __global__ void __launch_bounds__(256, MINB) fourier_pass_kernel(const __grid_co
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const int f = 2 * (threadIdx.x + (h + k) * nt);
-        x[k] = *reinterpret_cast<const float4*>(P.v + tile_global(P, tile, f));
+        x[k] = *reinterpret_cast<const float4*>(P.v + (tile_global(P, tile, f) & P.amask));
       }
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
@@ -447,7 +454,8 @@ __global__ void __launch_bounds__(256, MINB) fourier_pass_kernel(const __grid_co
       a = cmulf(a, window_factor(wt, f));
       b = cmulf(b, window_factor(wt, f + 1));
     }
-    if (P.store) *reinterpret_cast<float4*>(P.v + g) = make_float4(a.x, a.y, b.x, b.y);
+    if (P.store && (P.store_top < 0 || (int)((g >> (P.m - 1)) & 1ull) == P.store_top))
+      *reinterpret_cast<float4*>(P.v + (g & P.amask)) = make_float4(a.x, a.y, b.x, b.y);
     if (P.masses) mass = fmaf(a.x, a.x, fmaf(a.y, a.y, fmaf(b.x, b.x, fmaf(b.y, b.y, mass))));
   }
   if (P.masses) {
@@ -459,7 +467,7 @@ __global__ void __launch_bounds__(256, MINB) fourier_pass_kernel(const __grid_co
     if (threadIdx.x == 0) {
       double s = 0.0;
       for (int w = 0; w < (nt + 31) / 32; ++w) s += red[w];
-      P.masses[tile] = s;
+      P.masses[tile - P.tile0] = s;
     }
   }
 }
@@ -654,6 +662,14 @@ __global__ void __launch_bounds__(1024) fourier_draw_kernel(const double* __rest
   }
 }
 
+// Total of the tile masses of a shard (the same fixed-order reduction as the draw).
+__global__ void __launch_bounds__(1024) shard_mass_kernel(const double* __restrict__ masses, long long ntiles,
+                                                          double* __restrict__ out) {
+  double tot;
+  block_search(ntiles, 0.0, [&](long long i) { return masses[i]; }, &tot);
+  if (threadIdx.x == 0) *out = tot;
+}
+
 // ------------------------------------------------------------------------------------- host
 std::mutex g_fourier_mutex;
 
@@ -673,7 +689,7 @@ int set_smem_attr() {
 int launch_pass(const PassParams& P, cudaStream_t s) {
   const int TB = P.c + P.K;
   if (TB < 4 || TB > kTileBits) return fail(RGS_ERR_UNSUPPORTED, "tile must span 4..13 bits");
-  const u64 tiles = 1ull << (P.m - TB);
+  const u64 tiles = P.ntiles ? P.ntiles : (1ull << (P.m - TB));
   const size_t smem = ((1 << TB) + (1 << (TB - 4))) * sizeof(float2);
   int rc = P.variant ? set_smem_attr<4>() : set_smem_attr<3>();
   if (rc) return rc;
@@ -705,6 +721,8 @@ std::vector<std::pair<int, int>> strided_groups(int m) {
 PassParams base_params(const FourierPlan& p, float2* v) {
   PassParams P{};
   P.v = v;
+  P.amask = ~0ull;
+  P.store_top = -1;
   P.m = p.m;
   P.chunks = p.chunks;
   P.lut_a = (const u64*)p.d_lut_a;
@@ -725,6 +743,23 @@ void strided(PassParams& P, int lo, int hi) {
   P.K = hi - lo;
   P.c = kTileBits - P.K;
   P.q = lo;
+}
+
+// Two-shard schedule: the bits [11, m - 1) in balanced groups of at most 9 bits (bit
+// 11 is not in the shard's init tile, which holds bits 0..10 and the top bit m - 1).
+std::vector<std::pair<int, int>> shard_groups(int m) {
+  std::vector<std::pair<int, int>> g;
+  const int lo0 = kTileBits - 1, rest = (m - 1) - lo0;
+  if (rest <= 0) return g;
+  const int maxk = kTileBits - kLowBits;
+  const int k = (rest + maxk - 1) / maxk;
+  int lo = lo0;
+  for (int i = 0; i < k; ++i) {
+    const int size = rest / k + (i < rest % k ? 1 : 0);
+    g.push_back({lo, lo + size});
+    lo += size;
+  }
+  return g;
 }
 
 unsigned target_mask(const PassParams& P) { return ((1u << P.K) - 1u) << P.c; }
@@ -987,6 +1022,15 @@ std::string fourier_build(int n, const uint8_t* graph, const double* unitaries, 
     }
   }
   p.ngroups = (int)strided_groups(m).size();
+  // Two-shard schedule tables (see fourier_compute_shard).
+  p.shardable = deferred && m >= kTileBits + 1;
+  if (p.shardable) {
+    std::vector<u64h> qs;
+    pass_tables(p.lut_z, p.chunks, m, kTileBits - 1, 1, m - 1, true, p.tt_init_shard, qs);
+    const auto g = shard_groups(m).back();
+    const int K = g.second - g.first;
+    pass_tables(p.lut_a, p.chunks, m, kTileBits - K, K, g.first, false, p.tt_phase_shard, qs);
+  }
   status = RGS_OK;
   return "";
 }
@@ -1025,6 +1069,10 @@ int fourier_upload(FourierPlan& p, int device) {
   if ((rc = up(&p.d_uB, p.uB.data(), p.uB.size() * 8))) return rc;
   if ((rc = up(&p.d_tt_init, &p.tt_init, sizeof(TileTables)))) return rc;
   if ((rc = up(&p.d_tt_phase, &p.tt_phase, sizeof(TileTables)))) return rc;
+  if (p.shardable) {
+    if ((rc = up(&p.d_tt_init_shard, &p.tt_init_shard, sizeof(TileTables)))) return rc;
+    if ((rc = up(&p.d_tt_phase_shard, &p.tt_phase_shard, sizeof(TileTables)))) return rc;
+  }
   if ((rc = up(&p.d_qsym_z, p.qsym_z.data(), p.qsym_z.size() * 8))) return rc;
   if ((rc = up(&p.d_qsym_a, p.qsym_a.data(), p.qsym_a.size() * 8))) return rc;
   if (p.rot_ok) {
@@ -1128,6 +1176,121 @@ int fourier_compute(FourierPlan& p, uint64_t outB, void* state, void* ws, size_t
     cudaEventElapsedTime(&stages->product_ms, ev[2], ev[3]);
     for (auto& e : ev) cudaEventDestroy(e);
   }
+  return RGS_OK;
+}
+
+// Shard `shard` of two: the top bit m - 1 is the device index.  Pass schedule:
+//   pass 0        : tile = bits 0..10 and bit m - 1 (c = 11, K = 1, q = m - 1); the init is
+//                   computed for both values of the top bit and the WHT runs on all 12
+//                   tile bits, so the top bit's Walsh factor needs no exchange; only the
+//                   elements of this shard are stored
+//   strided passes: WHT on the groups of bits [11, m - 1) (this shard's tiles only)
+//   middle pass   : WHT on the last group, q_A phase (global index), products on it
+//   strided passes: products on the earlier groups, reverse order
+//   last pass     : products on bits 0..10 (contiguous tile of 12 bits) + tile masses
+// The products skip the top bit (its unitary is the deferred terminal one, applied at
+// draw time to the pair of values at one local index on the two shards).
+int fourier_compute_shard(FourierPlan& p, uint64_t outB, int shard, void* state, void* ws, size_t ws_bytes,
+                          cudaStream_t s) {
+  if (shard != 0 && shard != 1) return fail(RGS_ERR_ARG, "shard must be 0 or 1");
+  if (!p.shardable) return fail(RGS_ERR_UNSUPPORTED, "two-shard schedule needs the deferred sampler and m >= 13");
+  FourierLayout L;
+  int rc = check_state(p, state, ws, ws_bytes, L);
+  if (rc) return rc;
+  char* w = (char*)ws;
+  if ((rc = build_weights(p, outB, w, L, p.specialized, true, s))) return rc;
+  const int m = p.m;
+  PassParams P = base_params(p, (float2*)state);
+  P.amask = (1ull << (m - 1)) - 1ull;
+  P.init = p.specialized ? INIT_COV_SPECIAL : INIT_COV_GENERIC;
+  P.lut_z = (const u64*)p.d_lut_z;
+  P.wgen = (const double2*)(w + L.off_weights);
+  P.wspec = (const double2*)(w + L.off_weights);
+  P.wspecf = (const float2*)(w + L.off_wspecf);
+  P.outmask = outB;
+  P.rg = (const float2*)p.d_rg;
+  P.rh = (const float2*)p.d_rh;
+  if (p.specialized) {
+    P.tt_init = (const TileTables*)p.d_tt_init_shard;
+    P.qsym_z = (const u64*)p.d_qsym_z;
+  }
+  P.tt_phase = (const TileTables*)p.d_tt_phase_shard;
+  P.qsym_a = (const u64*)p.d_qsym_a;
+  P.variant = p.variant;
+  const float2* dg = p.rot_ok ? (const float2*)p.d_dg : nullptr;
+  const float2* dh = p.rot_ok ? (const float2*)p.d_dh : nullptr;
+  P.rot = p.rot_ok ? (const float2*)p.d_rot : nullptr;
+  // Pass 0: every tile of the index space, this shard's half of each stored.
+  P.c = kTileBits - 1;
+  P.K = 1;
+  P.q = m - 1;
+  P.wht_mask = (1u << kTileBits) - 1u;
+  P.store_top = shard;
+  if ((rc = launch_pass(P, s))) return rc;
+  P.store_top = -1;
+  P.init = INIT_LOAD;
+  // Later passes: tiles of 12 bits that never hold bit m - 1; this shard's half of them.
+  const u64 half_tiles = 1ull << (m - kTileBits - 1);
+  P.tile0 = (u64)shard * half_tiles;
+  P.ntiles = half_tiles;
+  const auto groups = shard_groups(m);
+  const int k = (int)groups.size();
+  for (int i = 0; i + 1 < k; ++i) {
+    strided(P, groups[i].first, groups[i].second);
+    P.wht_mask = target_mask(P);
+    if ((rc = launch_pass(P, s))) return rc;
+  }
+  strided(P, groups[k - 1].first, groups[k - 1].second);
+  P.wht_mask = target_mask(P);
+  P.phase = 1;
+  P.dg = dg;
+  P.u_mask = product_mask(p, P, target_mask(P));
+  if ((rc = launch_pass(P, s))) return rc;
+  P.phase = 0;
+  P.dg = nullptr;
+  P.wht_mask = 0;
+  for (int i = k - 2; i >= 0; --i) {
+    strided(P, groups[i].first, groups[i].second);
+    P.u_mask = product_mask(p, P, target_mask(P));
+    if ((rc = launch_pass(P, s))) return rc;
+  }
+  contiguous(P, m);
+  P.u_mask = product_mask(p, P, (1u << (kTileBits - 1)) - 1u);
+  P.dh = dh;
+  P.masses = (double*)(w + L.off_masses);
+  return launch_pass(P, s);
+}
+
+int fourier_shard_mass(FourierPlan& p, void* ws, double* mass, cudaStream_t s) {
+  if (!ws || !mass) return fail(RGS_ERR_ARG, "null workspace or output");
+  FourierLayout L;
+  fourier_layout(p, L);
+  char* w = (char*)ws;
+  double* d = (double*)(w + L.off_result);
+  shard_mass_kernel<<<1, 1024, 0, s>>>((const double*)(w + L.off_masses), L.ntiles / 2, d);
+  RGS_CUDA_TRY(cudaGetLastError());
+  RGS_CUDA_TRY(cudaMemcpyAsync(mass, d, sizeof(double), cudaMemcpyDeviceToHost, s));
+  RGS_CUDA_TRY(cudaStreamSynchronize(s));
+  return RGS_OK;
+}
+
+int fourier_shard_draw(FourierPlan& p, const void* state, void* ws, double u1, double u2, uint64_t* local_index,
+                       cudaStream_t s) {
+  FourierLayout L;
+  int rc = check_state(p, state, ws, (size_t)-1, L);
+  if (rc) return rc;
+  if (!local_index) return fail(RGS_ERR_ARG, "null output");
+  if (!(u1 >= 0.0 && u1 < 1.0 && u2 >= 0.0 && u2 < 1.0)) return fail(RGS_ERR_ARG, "uniforms must lie in [0, 1)");
+  char* w = (char*)ws;
+  DrawResult* d = (DrawResult*)(w + L.off_result);
+  fourier_draw_kernel<<<1, 1024, 0, s>>>((const double*)(w + L.off_masses), L.ntiles / 2, (const float2*)state,
+                                         p.m - 1, kTileBits, 0, nullptr, u1, u2, 0.0, d);
+  RGS_CUDA_TRY(cudaGetLastError());
+  DrawResult h;
+  RGS_CUDA_TRY(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, s));
+  RGS_CUDA_TRY(cudaStreamSynchronize(s));
+  if (h.status || !(h.norm > 0.0) || !std::isfinite(h.norm)) return fail(RGS_ERR_ZERO_NORM, "shard has no mass");
+  *local_index = h.index;
   return RGS_OK;
 }
 
@@ -1260,6 +1423,8 @@ int fwht_bits(void* state, int nbits, int lo, int hi, cudaStream_t s) {
   if (rc) return rc;
   PassParams P{};
   P.v = (float2*)state;
+  P.amask = ~0ull;
+  P.store_top = -1;
   P.store = 1;
   return transform_range(P, nbits, lo, hi, true, s);
 }
@@ -1271,6 +1436,8 @@ int product_bits(void* state, int nbits, const double* u_dev, int lo, int hi, cu
   if (!u_dev) return fail(RGS_ERR_ARG, "unitaries are required");
   PassParams P{};
   P.v = (float2*)state;
+  P.amask = ~0ull;
+  P.store_top = -1;
   P.store = 1;
   P.u = (const double2*)u_dev;
   return transform_range(P, nbits, lo, hi, false, s);

@@ -43,6 +43,10 @@ struct FourierPlan {
   std::vector<float> dg, dh;     // [chunks][256][2] complex64 chunk products of g / h
   std::vector<float> rg, rh;     // [m][2] per-bit ratios g(1)/g(0), h(1)/h(0)
   TileTables tt_init{}, tt_phase{};         // pass tables of the init (pass 0) and of the q_A phase pass
+  // Two-shard schedule (top bit m - 1 split over two devices, m >= 13): pass tables of the
+  // shard init pass (bits 0..10 plus bit m - 1) and of its q_A phase pass.
+  bool shardable = false;
+  TileTables tt_init_shard{}, tt_phase_shard{};
   std::vector<unsigned long long> qsym_z, qsym_a;  // [m] rows of Q + Q^T of the two phases
   // Pass schedule (see fourier.cu).
   int ngroups = 0;               // strided target groups above the low tile
@@ -60,6 +64,8 @@ struct FourierPlan {
   void* d_rh = nullptr;          // float2 [m]
   void* d_tt_init = nullptr;
   void* d_tt_phase = nullptr;
+  void* d_tt_init_shard = nullptr;
+  void* d_tt_phase_shard = nullptr;
   void* d_qsym_z = nullptr;
   void* d_qsym_a = nullptr;
   ~FourierPlan();
@@ -105,6 +111,17 @@ int fourier_index_map(FourierPlan& p, const void* src, void* dst, cudaStream_t s
 int fourier_quadphase(FourierPlan& p, void* state, cudaStream_t s);
 
 // Building blocks on a state of 2^nbits complex64 values (in place).
+// One half of the conditional state (top bit m - 1 == shard, shard in {0, 1}) on this
+// device: 2^(m-1) values at state, the deferred terminal unitary not applied, tile masses
+// of the half in the workspace.  The Walsh factor of the top bit is folded into the init
+// (both halves' initial values are computed, no exchange); every other operation is local.
+int fourier_compute_shard(FourierPlan& p, uint64_t outB, int shard, void* state, void* ws, size_t ws_bytes,
+                          cudaStream_t s);
+// Total mass of a computed shard (sum of its tile masses, fixed order).
+int fourier_shard_mass(FourierPlan& p, void* ws, double* mass, cudaStream_t s);
+// Two-level draw inside a computed shard (u1: tile, u2: element): the local index.
+int fourier_shard_draw(FourierPlan& p, const void* state, void* ws, double u1, double u2, uint64_t* local_index,
+                       cudaStream_t s);
 int fwht_bits(void* state, int nbits, int lo, int hi, cudaStream_t s);
 // The same butterflies with 16 x 16 Hadamard blocks on the tensor cores over `terms` (2
 // or 3) BF16 parts of each value (wht_tc.cu); nbits >= 12.

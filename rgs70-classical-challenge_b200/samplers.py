@@ -24,7 +24,8 @@ import torch
 
 from . import _lib
 
-__all__ = ["ConditionalSampler", "fwht", "product", "block_mass", "produce", "DrawRecorder", "cut_tables"]
+__all__ = ["ConditionalSampler", "ShardedConditionalSampler", "shard_choice", "terminal_pick", "draw_across_shards",
+           "draw_distributed", "fwht", "product", "block_mass", "produce", "DrawRecorder", "cut_tables"]
 
 
 def _stream(device):
@@ -218,6 +219,144 @@ class ConditionalSampler:
     def tables(self):
         """GF(2) lookup tables (covariant map, q_A phase, index map) and the rows of N."""
         return _tables(self._h, self.m)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().rgs_fourier_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
+# ---------------------------------------------------------------------- two shards
+def shard_choice(totals, u1):
+    """First level of a draw over shards laid end to end: the shard holding the point
+    u1 * sum(totals) of the cumulative mass, and the uniform rescaled to that shard's own
+    mass (the reference draws one tile index over the concatenated masses of both
+    devices, ``distributed_sampler.py:153-157``).  Returns (shard, u1 within it, norm)."""
+    totals = [float(t) for t in totals]
+    norm = sum(totals)
+    if not (norm > 0.0) or not np.isfinite(norm):
+        raise ArithmeticError(f"invalid shard masses {totals}")
+    target = u1 * norm
+    acc = 0.0
+    last = max(i for i, t in enumerate(totals) if t > 0.0)
+    for i, t in enumerate(totals):
+        if t > 0.0 and (target < acc + t or i == last):
+            return i, min(max((target - acc) / t, 0.0), np.nextafter(1.0, 0.0)), norm
+        acc += t
+    raise AssertionError("unreachable")
+
+
+def terminal_pick(pair, unitary, u3):
+    """The deferred terminal unitary on the two values at one local index (one per shard)
+    and the output bit (``deferred_global_sampler.py:65-78``): (bit, |(U pair)_bit|^2)."""
+    out = np.asarray(unitary, dtype=np.complex128) @ np.asarray(pair, dtype=np.complex128)
+    p = np.abs(out) ** 2
+    total = float(p.sum())
+    if not (total > 0.0) or not np.isfinite(total):
+        raise ArithmeticError("Invalid transformed local mass")
+    bit = int(u3 * total >= p[0])
+    return bit, float(p[bit])
+
+
+def draw_across_shards(shards, unitary, u1, u2, u3):
+    """One exact draw from two shards held in this process (objects with ``mass()``,
+    ``local_draw(u1, u2)``, ``value(local)`` and ``half``): shard by mass, local index by
+    the shard's two-level inverse CDF, bit by the terminal pair.  Returns (index, pa, norm)."""
+    s, u1s, norm = shard_choice([sh.mass() for sh in shards], u1)
+    local = shards[s].local_draw(u1s, u2)
+    bit, pa = terminal_pick([sh.value(local) for sh in shards], unitary, u3)
+    return bit * shards[0].half + local, pa, norm
+
+
+def draw_distributed(shard, unitary, rng, rank, group=None, device=None):
+    """The same draw with one shard per process (rank = shard index, two ranks): rank 0
+    draws the three uniforms (the reference's RNG call order) and broadcasts them; the two
+    shard masses, the chosen local index and the two terminal values are the only data
+    exchanged (collectives on `device` tensors: CPU for gloo, CUDA for NCCL).
+    Returns (index, pa, norm) on every rank."""
+    import torch.distributed as dist
+    dev = device if device is not None else torch.device("cpu")
+    u = torch.zeros(3, dtype=torch.float64, device=dev)
+    if rank == 0:
+        u[:] = torch.tensor([float(rng.random()), float(rng.random()), float(rng.random())], dtype=torch.float64)
+    dist.broadcast(u, src=0, group=group)
+    u1, u2, u3 = (float(x) for x in u.cpu())
+    masses = [torch.zeros(1, dtype=torch.float64, device=dev) for _ in range(2)]
+    dist.all_gather(masses, torch.tensor([shard.mass()], dtype=torch.float64, device=dev), group=group)
+    s, u1s, norm = shard_choice([float(m.item()) for m in masses], u1)
+    loc = torch.zeros(1, dtype=torch.int64, device=dev)
+    if rank == s:
+        loc[0] = int(shard.local_draw(u1s, u2))
+    dist.broadcast(loc, src=s, group=group)
+    local = int(loc.item())
+    v = shard.value(local)
+    vals = [torch.zeros(2, dtype=torch.float64, device=dev) for _ in range(2)]
+    dist.all_gather(vals, torch.tensor([v.real, v.imag], dtype=torch.float64, device=dev), group=group)
+    pair = [complex(float(t[0]), float(t[1])) for t in vals]
+    bit, pa = terminal_pick(pair, unitary, u3)
+    return bit * shard.half + local, pa, norm
+
+
+class ShardedConditionalSampler:
+    """One of two shards of the conditional state on this device: the values whose top A
+    bit equals ``shard`` (2^(m-1) complex64), the deferred terminal unitary not applied
+    (``DeferredGlobalMixin``, ``W/deferred_global_sampler.py:40-88``).  The top bit's Walsh
+    factor is folded into the initialisation, so computing a shard needs no data from the
+    other one; a draw exchanges two scalars per shard (``draw_distributed``), or runs on
+    two shards of one process (``draw_across_shards``).  m >= 13."""
+
+    def __init__(self, g, u, A, B, shard, device=0):
+        g = np.ascontiguousarray(np.asarray(g, dtype=np.uint8))
+        u = np.ascontiguousarray(np.asarray(u, dtype=np.complex128))
+        self.A, self.B = [int(a) for a in A], [int(b) for b in B]
+        self.m = len(self.A)
+        if shard not in (0, 1):
+            raise ValueError("shard must be 0 or 1")
+        self.shard = shard
+        self.device = torch.device("cuda", device) if isinstance(device, int) else torch.device(device)
+        self._h = _create(g, u, self.A, self.B, True)
+        self.half = 1 << (self.m - 1)
+        ws = ctypes.c_size_t()
+        _lib.check(_lib.lib().rgs_fourier_workspace_bytes(self._h, ctypes.byref(ws)))
+        with torch.cuda.device(self.device):
+            self.state = torch.empty(self.half, dtype=torch.complex64, device=self.device)
+            self.workspace = torch.empty(ws.value, dtype=torch.uint8, device=self.device)
+        self.terminal_unitary = np.asarray(u[self.A[-1]], dtype=np.complex128)
+
+    def compute(self, outB):
+        bits = np.asarray(outB)
+        if bits.shape != (self.m,) or np.any((bits != 0) & (bits != 1)):
+            raise ValueError("outB must contain m bits")
+        mask = int(sum(int(x) << j for j, x in enumerate(bits)))
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.lib().rgs_fourier_compute_shard(
+                self._h, mask, self.shard, ctypes.c_void_p(self.state.data_ptr()),
+                ctypes.c_void_p(self.workspace.data_ptr()), self.workspace.numel(), _stream(self.device)))
+
+    def mass(self):
+        out = ctypes.c_double()
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.lib().rgs_fourier_shard_mass(self._h, ctypes.c_void_p(self.workspace.data_ptr()),
+                                                         ctypes.byref(out), _stream(self.device)))
+        return float(out.value)
+
+    def local_draw(self, u1, u2):
+        idx = ctypes.c_uint64()
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.lib().rgs_fourier_shard_draw(self._h, ctypes.c_void_p(self.state.data_ptr()),
+                                                         ctypes.c_void_p(self.workspace.data_ptr()), float(u1),
+                                                         float(u2), ctypes.byref(idx), _stream(self.device)))
+        return int(idx.value)
+
+    def value(self, local):
+        return complex(self.state[int(local)].item())
+
+    def host(self):
+        return self.state.cpu().numpy().astype(np.complex128)
 
     def __del__(self):
         h = getattr(self, "_h", None)
