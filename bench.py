@@ -69,12 +69,25 @@ def step_bytes(ranks, esize, pairs=()):
     return esize * (total - sum(2 << ranks[j] for j in pairs))
 
 
-def chain_bytes(plan, esize):
-    """Compulsory table traffic of one chain-rule sample: the scan sweep, plus one read of
-    the input table of every position whose branch masses need the Gram pass (a
-    position with an empty kernel has them in closed form)."""
-    gram = sum((1 << st.r_in) for j, st in enumerate(plan.steps) if j > 0 and len(st.kernel) > 0)
-    return step_bytes(plan.ranks, esize) + esize * gram
+def chain_bytes(plan, esize, fused=True):
+    """Compulsory table traffic of one chain-rule sample: per position, one read of its input
+    table for the Gram pass (unless the branch masses are analytic: an empty kernel), one
+    read of the input and one write of the output for the step; per fused pair (j, j + 1):
+    the Gram read of j's input if j needs it, one more read of j's input for j + 1's Gram
+    matrix if j + 1 needs it, then one read of j's input and one write of j + 1's output."""
+    steps = plan.steps
+    pairs = set(plan.pairs) if fused else set()
+    total, j = 0, 0
+    while j < len(steps):
+        st = steps[j]
+        gram = j > 0 and len(st.kernel) > 0
+        if j in pairs and j + 1 < len(steps):
+            total += (1 << st.r_in) * (int(gram) + int(len(steps[j + 1].kernel) > 0) + 1) + (1 << steps[j + 1].r_out)
+            j += 2
+        else:
+            total += (1 << st.r_in) * (int(gram) + int(j > 0)) + (1 << st.r_out)
+            j += 1
+    return esize * total
 
 
 def reference_bytes(ranks, esize):

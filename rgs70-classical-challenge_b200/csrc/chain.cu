@@ -14,6 +14,13 @@
 //                         log p(x_v | prefix), and the weights of the chosen branch
 //   scan step kernel    : the chosen branch, with the usual power-of-two renormalisation
 // so a sample costs one scan sweep plus one read of the tables of the other positions.
+// Fused pairs of the plan (positions j, j + 1; complex64 tables with float64 arithmetic
+// and complex128): x_j as above; then one pass over j's input forms j's outputs in
+// registers and accumulates the Gram matrix of position j + 1 (scan_pair_kernel, GRAM
+// mode, no stores) unless j + 1 is analytic; x_{j+1}; then the pair kernel writes the
+// output of j + 1.  The table between the two positions never reaches memory: per pair
+// 2 reads of j's input and 1 write instead of 1 read, 3 passes over the intermediate
+// table and 1 write.
 // The final table is the amplitude of the drawn string, returned like rgs_scan_amplitudes.
 #include <cuda_runtime.h>
 
@@ -333,28 +340,61 @@ int chain_run(Plan& plan, const double* U, long long count, int mode_given, u64 
   int* status = (int*)(ws + L.off_status);
   const u64* tables = (const u64*)dc->tables;
   const double2* U2 = (const double2*)U;
+  // Fused pairs of positions (the plan's pairs) for complex64 tables with float64
+  // arithmetic and for complex128.
+  const bool fuse = (precision == RGS_PREC_C64 || precision == RGS_PREC_C128) && !plan.pair_at.empty();
   RGS_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), stream));
   for (long long first = 0; first < count; first += Bt) {
     const int cnt = (int)std::min<long long>(Bt, count - first);
     if (!mode_given) chain_clear_bits_kernel<<<(cnt + 127) / 128, 128, 0, stream>>>(bits, first, cnt);
     if (out_logp) chain_zero_kernel<<<(cnt + 127) / 128, 128, 0, stream>>>(out_logp, first, cnt);
     RGS_CUDA_TRY(cudaMemsetAsync(maxbuf, 0, (size_t)plan.n * Bt * sizeof(u64), stream));
-    for (int j = 0; j < plan.n; ++j) {
+    // Branch masses of position j (the Gram pass over its input, unless analytic), then
+    // the choice of x_{v_j} and the chosen branch's weights.
+    auto decide = [&](int j, const void* in) -> cudaError_t {
       const DevStep& st = plan.dev[j];
-      const int v = st.v;
       const int analytic = (st.mode == MODE_PAIR && st.ncombos == 1) ? 1 : 0;
-      if (!analytic)
-        RGS_CUDA_TRY(launch_gram_step(precision, Bt, L.mass_blocks, stream, buf[j & 1], st, tables + st.table_off,
-                                      partial, j == 0));
+      if (!analytic && in) {
+        cudaError_t e = launch_gram_step(precision, Bt, L.mass_blocks, stream, in, st, tables + st.table_off, partial,
+                                         j == 0);
+        if (e != cudaSuccess) return e;
+      }
       chain_decide_kernel<<<(Bt * 32 + 127) / 128, 128, 0, stream>>>(
-          partial, L.mass_blocks, analytic, Bt, cnt, j, v, U2, mode_given, bits, first, uniforms, plan.n, seed,
+          partial, L.mass_blocks, analytic, Bt, cnt, j, st.v, U2, mode_given, bits, first, uniforms, plan.n, seed,
           W + (size_t)j * Bt, out_logp, out_cond1, status);
-      RGS_CUDA_TRY(cudaGetLastError());
-      RGS_CUDA_TRY(scan_launch_step(precision, Bt, device, st, buf[j & 1], buf[(j + 1) & 1], tables + st.table_off,
-                                    W + (size_t)j * Bt, nullptr, j ? maxbuf + (size_t)(j - 1) * Bt : nullptr,
-                                    maxbuf + (size_t)j * Bt, j == 0, stream));
+      return cudaGetLastError();
+    };
+    int seg = 0;
+    for (int j = 0; j < plan.n; ++seg) {
+      const void* in = buf[seg & 1];
+      void* out = buf[(seg + 1) & 1];
+      const int pa = fuse ? plan.pair_at[j] : -1;
+      if (pa >= 0 && j + 1 < plan.n) {
+        // Fused pair (j, j + 1): x_j as usual; B's branch masses from a pass over j's
+        // input that forms j's outputs in registers (nothing written); x_{j+1}; then the
+        // pair kernel writes B's output.  j's output table never reaches memory.
+        const DevPair& P = plan.pairs[pa];
+        const DevStep& sb = plan.dev[j + 1];
+        const bool analytic_b = sb.mode == MODE_PAIR && sb.ncombos == 1;
+        RGS_CUDA_TRY(decide(j, in));
+        if (!analytic_b)
+          RGS_CUDA_TRY(scan_launch_pair_gram(precision, Bt, L.mass_blocks, P, in, tables, W + (size_t)j * Bt,
+                                             maxbuf + (size_t)(j - 1) * Bt, partial, stream));
+        RGS_CUDA_TRY(decide(j + 1, nullptr));
+        RGS_CUDA_TRY(scan_launch_pair(precision, Bt, device, P, in, out, tables, W + (size_t)j * Bt,
+                                      W + (size_t)(j + 1) * Bt, maxbuf + (size_t)(j - 1) * Bt, maxbuf + (size_t)j * Bt,
+                                      maxbuf + (size_t)(j + 1) * Bt, stream));
+        j += 2;
+      } else {
+        const DevStep& st = plan.dev[j];
+        RGS_CUDA_TRY(decide(j, in));
+        RGS_CUDA_TRY(scan_launch_step(precision, Bt, device, st, in, out, tables + st.table_off, W + (size_t)j * Bt,
+                                      nullptr, j ? maxbuf + (size_t)(j - 1) * Bt : nullptr, maxbuf + (size_t)j * Bt,
+                                      j == 0, stream));
+        j += 1;
+      }
     }
-    RGS_CUDA_TRY(scan_launch_finalize(precision, buf[plan.n & 1], maxbuf, plan.n, Bt, cnt,
+    RGS_CUDA_TRY(scan_launch_finalize(precision, buf[seg & 1], maxbuf, plan.n, Bt, cnt,
                                       (char*)out_value + (size_t)first * (precision == RGS_PREC_C128 ? 16 : 8),
                                       out_logscale + first, stream));
   }

@@ -397,6 +397,30 @@ cudaError_t launch_pair(int precision, int Bt, int device, cudaStream_t s, const
   return launch_pair_f32(VE, grid, s, Ein, Eout, P, tables, WA, WB, mp, mA, mc, lbt, es);
 }
 
+}  // namespace
+
+cudaError_t scan_launch_pair(int precision, int Bt, int device, const DevPair& P, const void* Ein, void* Eout,
+                             const u64* tables, const double4* WA, const double4* WB, const u64* mp, u64* mA, u64* mc,
+                             cudaStream_t s) {
+  return launch_pair(precision, Bt, device, s, Ein, Eout, P, tables, WA, WB, mp, mA, mc);
+}
+
+cudaError_t scan_launch_pair_gram(int precision, int Bt, int blocks, const DevPair& P, const void* Ein,
+                                  const u64* tables, const double4* WA, const u64* mp, double* partial,
+                                  cudaStream_t s) {
+  const int lbt = __builtin_ctz((unsigned)Bt);
+  const int VE = (precision != RGS_PREC_C128 && Bt >= 2) ? 2 : 1;
+  const int lC = lbt - (VE == 2 ? 1 : 0);
+  const int lL = lC < 5 ? lC : 5;
+  if (lC - lL > 3) return cudaErrorInvalidValue;  // more column slices than warps in a block
+  const dim3 grid((unsigned)blocks);
+  if (precision == RGS_PREC_C128) return launch_pair_gram_c128(VE, grid, s, Ein, P, tables, WA, mp, lbt, partial);
+  if (precision == RGS_PREC_C64) return launch_pair_gram_c64(VE, grid, s, Ein, P, tables, WA, mp, lbt, partial);
+  return cudaErrorInvalidValue;
+}
+
+namespace {
+
 // The sweep as segments: one position, or a fused pair (plan.pair_at).
 struct Segment {
   int j, len, pair;

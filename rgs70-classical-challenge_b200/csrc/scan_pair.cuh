@@ -76,12 +76,17 @@ struct PairBlocks {
   static constexpr int value = sizeof(M) > sizeof(S) ? 1 : RGS_PAIR_MINB;
 };
 
-template <typename S, typename M, int VE, int CA, int CB, typename I>
+// GRAM = true (chain-rule sampling, the first of two passes over a pair): instead of B's
+// outputs, the 2x2 Gram matrix of B's branch masses per item (see chain.cu) from the
+// group's intermediate rows, nothing stored; per-block partials (G00, G11, Re G01,
+// Im G01) of every item go to partial[block][item][4] (dynamic shared memory: 8 warps x
+// Bt x 4 doubles).  B's weights are not read.
+template <typename S, typename M, int VE, int CA, int CB, typename I, bool GRAM = false>
 __global__ void __launch_bounds__(256, PairBlocks<S, M>::value)
     scan_pair_kernel(const S* __restrict__ Ein, S* __restrict__ Eout, const __grid_constant__ DevPair P,
                      const u64* __restrict__ tables, const double4* __restrict__ WA, const double4* __restrict__ WB,
                      const u64* __restrict__ maxprev, u64* __restrict__ maxA, u64* __restrict__ maxcur, int lbt,
-                     u64 e_stride) {
+                     u64 e_stride, double* __restrict__ partial) {
   using MA = PairMode<CA>;
   using MB = PairMode<CB>;
   constexpr int NCA = MA::nc, NCB = MB::nc;
@@ -113,9 +118,11 @@ __global__ void __launch_bounds__(256, PairBlocks<S, M>::value)
     maxA += k << lbt;
     maxcur += k << lbt;
   }
-  for (int i = threadIdx.x; i < Bt; i += blockDim.x) smax[i] = 0;
-  if (blockIdx.x == 0)
-    for (int i = threadIdx.x; i < Bt; i += blockDim.x) maxA[i] = max_bits<S>((S)0.25);
+  if (!GRAM) {
+    for (int i = threadIdx.x; i < Bt; i += blockDim.x) smax[i] = 0;
+    if (blockIdx.x == 0)
+      for (int i = threadIdx.x; i < Bt; i += blockDim.x) maxA[i] = max_bits<S>((S)0.25);
+  }
 
   const u64 gwarp = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
@@ -127,7 +134,7 @@ __global__ void __launch_bounds__(256, PairBlocks<S, M>::value)
   for (int v = 0; v < VE; ++v) {
     const int b = (int)(col * VE) + v;
     const double s = ldexp(1.0, -scale_exponent(max_value<S>(maxprev[b])));
-    const double4 fa = WA[b], fb = WB[b];
+    const double4 fa = WA[b], fb = GRAM ? WA[b] : WB[b];
     double ar = fa.x * s, ai = fa.y * s, br = fa.z * s, bi = fa.w * s;
     if (!MA::pair) {
       const double pr = ar + br, pi = ai + bi, mr = ar - br, mi = ai - bi;
@@ -151,8 +158,12 @@ __global__ void __launch_bounds__(256, PairBlocks<S, M>::value)
   const u64 per_iter = (u64)U << lR;
   const u64 wslice = nwarps >> lS;  // warps per column slice
   S mx[VE];
+  double gacc[VE][4];  // GRAM: Gram partials per item
 #pragma unroll
-  for (int v = 0; v < VE; ++v) mx[v] = (S)0;
+  for (int v = 0; v < VE; ++v) {
+    mx[v] = (S)0;
+    gacc[v][0] = gacc[v][1] = gacc[v][2] = gacc[v][3] = 0.0;
+  }
   // A warp iteration takes the groups base | idx, idx < per_iter (base a multiple of
   // per_iter).  q0 (zeros deposited at W's pivots), both table maps and the parity of
   // q0 & beta_B are GF(2)-linear in the group index, so the part of idx comes from this
@@ -234,6 +245,42 @@ __global__ void __launch_bounds__(256, PairBlocks<S, M>::value)
             ii[a] = (S)x.im;
           }
         }
+        if constexpr (GRAM) {
+          // Every output of B is alpha f(0) + beta f(1): PAIR B, output X: alpha = the
+          // kappa-0 rows, beta = the others with their signs, output Y the mirror image;
+          // MERGE B: alpha = all rows, beta = all rows with their signs.
+#pragma unroll
+          for (int b = 0; b < NUB; ++b) {
+            double axr = 0.0, axi = 0.0, bxr = 0.0, bxi = 0.0, ayr = 0.0, ayi = 0.0, byr = 0.0, byi = 0.0;
+#pragma unroll
+            for (int a = 0; a < NCB; ++a) {
+              const int i = MA::pair ? (a << 1) | b : a;
+              const int par = pq[u] ^ (int)((P.pwB >> i) & 1u);
+              const double er = (double)ir[i], ei = (double)ii[i];
+              const double nr = par ? -er : er, ni = par ? -ei : ei;
+              if (MB::pair) {
+                if (a < MB::ng0) {
+                  axr += er, axi += ei, byr += nr, byi += ni;
+                } else {
+                  bxr += nr, bxi += ni, ayr += er, ayi += ei;
+                }
+              } else {
+                axr += er, axi += ei, bxr += nr, bxi += ni;
+              }
+            }
+            gacc[v][0] = fma(axr, axr, fma(axi, axi, gacc[v][0]));
+            gacc[v][1] = fma(bxr, bxr, fma(bxi, bxi, gacc[v][1]));
+            gacc[v][2] = fma(axr, bxr, fma(axi, bxi, gacc[v][2]));
+            gacc[v][3] = fma(axi, bxr, fma(-axr, bxi, gacc[v][3]));
+            if (MB::pair) {
+              gacc[v][0] = fma(ayr, ayr, fma(ayi, ayi, gacc[v][0]));
+              gacc[v][1] = fma(byr, byr, fma(byi, byi, gacc[v][1]));
+              gacc[v][2] = fma(ayr, byr, fma(ayi, byi, gacc[v][2]));
+              gacc[v][3] = fma(ayi, byr, fma(-ayr, byi, gacc[v][3]));
+            }
+          }
+          continue;
+        }
         // B: the group's output rows from the registers.
 #pragma unroll
         for (int b = 0; b < NUB; ++b) {
@@ -266,13 +313,46 @@ __global__ void __launch_bounds__(256, PairBlocks<S, M>::value)
           }
         }
       }
+      if (!GRAM) {
 #pragma unroll
-      for (int b = 0; b < NUB; ++b) {
-        const I cx = c0[u] ^ (I)P.MB0[b];
-        outX[b].store(Eout, (u64)(((I)cx << lC) | (I)col));
-        if (MB::pair) outY[b].store(Eout, (u64)(((I)(cx ^ (I)P.tB) << lC) | (I)col));
+        for (int b = 0; b < NUB; ++b) {
+          const I cx = c0[u] ^ (I)P.MB0[b];
+          outX[b].store(Eout, (u64)(((I)cx << lC) | (I)col));
+          if (MB::pair) outY[b].store(Eout, (u64)(((I)(cx ^ (I)P.tB) << lC) | (I)col));
+        }
       }
     }
+  }
+
+  if constexpr (GRAM) {
+    // Deterministic reduction: lanes of other groups that own the same column
+    // (shuffles), warps (shared memory, fixed order), one partial per block and item.
+    extern __shared__ double red[];  // [8 warps][Bt][4]
+    const int wib = threadIdx.x >> 5;
+#pragma unroll
+    for (int v = 0; v < VE; ++v)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        double a = gacc[v][q];
+        for (int off = 16; off >= (1 << lL); off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+        gacc[v][q] = a;
+      }
+    for (int i = threadIdx.x; i < 8 * Bt * 4; i += blockDim.x) red[i] = 0.0;
+    __syncthreads();
+    if (sub == 0)
+#pragma unroll
+      for (int v = 0; v < VE; ++v)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) red[((size_t)wib * Bt + (int)(col * VE) + v) * 4 + q] = gacc[v][q];
+    __syncthreads();
+    for (int b = threadIdx.x; b < Bt; b += blockDim.x)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        double t = 0.0;
+        for (int wv = 0; wv < (int)(blockDim.x >> 5); ++wv) t += red[((size_t)wv * Bt + b) * 4 + q];
+        partial[((size_t)blockIdx.x * Bt + b) * 4 + q] = t;
+      }
+    return;
   }
 
   // Maximum |E|^2 of B's outputs per item: lanes of other groups in the warp that own

@@ -11,4 +11,12 @@ cudaError_t launch_pair_c128(int VE, dim3 grid, cudaStream_t s, const void* Ein,
   return launch_pair_codes<double, double, 1>(grid, s, Ein, Eout, P, tables, WA, WB, mp, mA, mc, lbt, es);
 }
 
+// Chain-rule sampling: B's Gram partials from a pass over A's input (no stores).
+cudaError_t launch_pair_gram_c128(int VE, dim3 grid, cudaStream_t s, const void* Ein, const DevPair& P,
+                                    const u64* tables, const double4* WA, const u64* mp, int lbt, double* partial) {
+  (void)VE;
+  return launch_pair_codes<double, double, 1, true>(grid, s, Ein, nullptr, P, tables, WA, WA, mp, nullptr, nullptr,
+                                                    lbt, 0, partial);
+}
+
 }  // namespace rgs

@@ -11,4 +11,14 @@ cudaError_t launch_pair_c64(int VE, dim3 grid, cudaStream_t s, const void* Ein, 
   return launch_pair_codes<float, double, 2>(grid, s, Ein, Eout, P, tables, WA, WB, mp, mA, mc, lbt, es);
 }
 
+// Chain-rule sampling: B's Gram partials from a pass over A's input (no stores).
+cudaError_t launch_pair_gram_c64(int VE, dim3 grid, cudaStream_t s, const void* Ein, const DevPair& P,
+                                   const u64* tables, const double4* WA, const u64* mp, int lbt, double* partial) {
+  if (VE == 1)
+    return launch_pair_codes<float, double, 1, true>(grid, s, Ein, nullptr, P, tables, WA, WA, mp, nullptr, nullptr,
+                                                     lbt, 0, partial);
+  return launch_pair_codes<float, double, 2, true>(grid, s, Ein, nullptr, P, tables, WA, WA, mp, nullptr, nullptr,
+                                                   lbt, 0, partial);
+}
+
 }  // namespace rgs
