@@ -492,17 +492,24 @@ def run_ours(args, rank, world, local_rank):
             peak_extra = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"])
         del graphs
         torch.cuda.empty_cache()
-        fs, fs_inst = full_scale(pkg, device, 64, legs=("random_order",), rescore=64)
-        leg = fs["random_order"]
-        extra["full_scale_n70"] = dict(leg, workload="config 5: n=70 random degree<=3 graph, seeded random order "
-                                                     f"(r_max {leg['rmax']}), 64 exact Born samples by the chain rule",
-                                       instance=fs_inst.name, unit="samples/s",
-                                       hbm_frac=leg["achieved_GBps"] / peak_extra)
-        torch.cuda.empty_cache()
-        extra["learned_n56"] = learned_comparison(pkg, device, 1024, 1 << 16, 4)
-        torch.cuda.empty_cache()
-        extra["wht_fp32_vs_split_bf16"] = wht_precision_leg(pkg, device, peak_extra)
-        torch.cuda.empty_cache()
+
+        def full_leg():
+            fs, fs_inst = full_scale(pkg, device, 64, legs=("random_order",), rescore=64)
+            leg = fs["random_order"]
+            return dict(leg, workload="config 5: n=70 random degree<=3 graph, seeded random order "
+                                      f"(r_max {leg['rmax']}), 64 exact Born samples by the chain rule",
+                        instance=fs_inst.name, unit="samples/s", hbm_frac=leg["achieved_GBps"] / peak_extra)
+
+        # Each leg on its own: a failure is reported in the line, not fatal to it.
+        for key, fn in (("full_scale_n70", full_leg),
+                        ("learned_n56", lambda: learned_comparison(pkg, device, 1024, 1 << 16, 4)),
+                        ("wht_fp32_vs_split_bf16", lambda: wht_precision_leg(pkg, device, peak_extra))):
+            try:
+                extra[key] = fn()
+            except Exception as exc:
+                extra[key] = {"error": f"{type(exc).__name__}: {exc}"}
+            torch.cuda.synchronize(device)
+            torch.cuda.empty_cache()
     line = None
     if rank == 0:
         cpu = None

@@ -140,12 +140,16 @@ def test_learned_rejection_is_born_exact_with_envelope(pkg, trained):
     e = np.bincount(grp, weights=probs, minlength=G) * len(idx)
     c = np.bincount(grp[idx], minlength=G)
     assert stats.chi2.sf(((c - e) ** 2 / e).sum(), G - 1) > 1e-4
-    # Acceptance of the learned proposal under its exact envelope, next to the uniform
-    # proposal's (1 / max 2^n p); reported, not asserted: KL training fits the bulk of p,
-    # while the envelope is set by the worst ratio p/q.
+    # What the trained network gains over the method without it: exact rejection with a
+    # proposal q accepts 1 / max_x (p / q) of its proposals; with the uniform proposal
+    # that is 1 / (2^n max p), with the learned one 1 / exp(log_c) (both envelopes exact,
+    # computed over all 2^n strings, so the comparison carries no sampling noise).
     uniform_acc = 1.0 / ((2.0 ** n) * probs.max())
-    print(f"learned acceptance {st['acceptance']:.4f}, uniform acceptance {uniform_acc:.4f}")
-    assert st["acceptance"] > 0.5 / np.exp(log_c)
+    learned_acc = float(np.exp(-log_c))
+    print(f"learned acceptance {learned_acc:.4f} (measured {st['acceptance']:.4f}), "
+          f"uniform acceptance {uniform_acc:.4f}")
+    assert learned_acc > uniform_acc
+    assert abs(st["acceptance"] - learned_acc) < 5 * np.sqrt(learned_acc / st["proposals"]) + 0.01
     # An envelope below max p/q is reported as violations (output then follows min(p, cq)).
     _, _, st2 = pkg.proposal.rejection_sample(so.probabilities, propose, log_c - 2.0, 1000, rng)
     assert st2["envelope_violations"] > 0
