@@ -1106,6 +1106,11 @@ def learned_comparison(pkg, device, samples, train_samples, epochs, order_policy
     val_lq = net.log_q(torch.as_tensor(val_bits[:, order_a].astype(np.float32)).to(device)).cpu().numpy()
     deficit = float(np.mean(np.maximum(0.0, 1.0 - np.exp(log_c - (val_logp - val_lq)))))
     viol_val = int(np.sum(val_logp - val_lq > log_c))
+    # Envelopes calibrated the same way for the defensive mixture (1/2 network, 1/2
+    # uniform) and for the uniform proposal alone: acceptance = 1 / c.
+    log_c_mix, _ = pkg.calibrate_envelope(cal_logp, net.mixture_log_q(cal_lq, 0.5), quantile=1.0, slack=1.5)
+    log_c_uni, _ = pkg.calibrate_envelope(cal_logp, np.full(len(cal_logp), -n * math.log(2.0)), quantile=1.0,
+                                          slack=1.5)
 
     def propose(r):
         x, lq = net.sample(8192, seed=1000 + r)
@@ -1142,6 +1147,8 @@ def learned_comparison(pkg, device, samples, train_samples, epochs, order_policy
         "learned_over_plain": learned / chain,
         "envelope": {"log_c": log_c, "validation_deficit_tv": deficit, "validation_violations": viol_val,
                      "validation_samples": 16384},
+        "calibrated_acceptance": {"network": math.exp(-log_c), "mixture_half_uniform": math.exp(-log_c_mix),
+                                  "uniform": math.exp(-log_c_uni)},
         "training": {"exact_sample_seconds": t_data, "train_seconds": t_train, "loss_first": losses[0],
                      "loss_last": float(np.mean(losses[-5:])), "entropy_floor": floor,
                      "kl_estimate": float(np.mean(losses[-5:]) - floor)}}

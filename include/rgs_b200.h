@@ -315,6 +315,10 @@ int rgs_gemm_bf16(int32_t M, int32_t N, int32_t K, const void* A, int32_t lda, i
  * passes) gave up since the last call (its results are then invalid); clears the flag.
  * Synchronous. */
 int rgs_tensor_core_status(int32_t* timed_out);
+/* TMA loads of the GEMM's K-major operands with 16-byte aligned rows: on (1, default) or
+ * off (0: every operand staged by the threads).  Both paths issue the same MMAs in the
+ * same order; the switch exists for tests and measurements.  Process-wide. */
+int rgs_gemm_set_tma(int32_t on);
 /* Forward: x bf16[batch][n] -> h1, h2 bf16[batch][hidden] -> logits z fp32[batch][n];
  * weights bf16 W1[hidden][n], W2[hidden][hidden], W3[n][hidden] (already masked), biases fp32. */
 int rgs_mlp_fwd(int32_t batch, int32_t n, int32_t hidden, const void* x, const void* w1b, const float* b1,

@@ -82,6 +82,8 @@ int rgs_tensor_core_status(int32_t* timed_out) {
   return rc;
 }
 
+int rgs_gemm_set_tma(int32_t on) { return gemm_set_tma(on); }
+
 int rgs_mlp_fwd(int32_t batch, int32_t n, int32_t hidden, const void* x, const void* w1b, const float* b1,
                 const void* w2b, const float* b2, const void* w3b, const float* b3, void* h1b, void* h2b, float* z,
                 void* stream) {

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstring>
 
 #include "common.hpp"
 #include "made.hpp"
@@ -102,21 +103,34 @@ __device__ __forceinline__ void stage_tile(unsigned char* tile, const __nv_bfloa
   }
 }
 
+// TMA descriptors of the operands that are K-major with 16-byte aligned rows (boxes of
+// 64 K-elements x 128 rows, 128-byte swizzle); the others are staged by the threads.
+struct GemmMaps {
+  CUtensorMap a, b;
+  int tma_a, tma_b;
+};
+
 // C[M x N] = op(A)[M x K] * op(B)[K x N]; A row-major [M][lda] (transA: [K][lda]), B
-// row-major [K][ldb] (transB: [N][ldb]).  One CTA of 128 threads per 128 x 128 tile of C:
-// all threads stage a K-slice of both operands (double-buffered), thread 0 issues four
-// tcgen05.mma (K = 16 each) per slice into the TMEM accumulator and commits them to the
-// stage's mbarrier, which gates the reuse of that stage; after the last slice every warp
-// reads its 32 TMEM lanes (rows) and applies the epilogue.
-__global__ void __launch_bounds__(128) gemm_tc_kernel(GemmArgs g) {
+// row-major [K][ldb] (transB: [N][ldb]).  One CTA of 128 threads per 128 x 128 tile of C,
+// K in slices of 64 over two shared-memory stages.  Per slice: thread 0 starts the TMA
+// loads of the K-major aligned operands (one 64 x 128 box each, completing on the stage's
+// `full` mbarrier), the threads stage the other operands (MN-major operands transposed
+// in registers); thread 0 then waits for the TMA bytes, issues four tcgen05.mma (K = 16
+// each) into the TMEM accumulator and commits them to the stage's `done` mbarrier,
+// which gates the reuse of that stage.  After the last slice every warp reads its 32 TMEM
+// lanes (rows) and applies the epilogue.
+__global__ void __launch_bounds__(128) gemm_tc_kernel(GemmArgs g, const __grid_constant__ GemmMaps maps) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kStages * 2 * kTileBytes);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kStages);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kStages * 2 * kTileBytes);  // done[2], full[2]
+  uint64_t* full = bars + kStages;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.y * TBM, n0 = blockIdx.x * TBN;
+  const bool tma = maps.tma_a || maps.tma_b;
+  const uint32_t tx_bytes = (maps.tma_a ? kTileBytes : 0) + (maps.tma_b ? kTileBytes : 0);
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) tc::mbar_init(&bars[s], 1);
+    for (int s = 0; s < 2 * kStages; ++s) tc::mbar_init(&bars[s], 1);
     tc::fence_barrier_init();
   }
   if (warp == 0) tc::tmem_alloc(tmem_slot, TBN);
@@ -138,18 +152,33 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(GemmArgs g) {
     }
     unsigned char* As = base + s * 2 * kTileBytes;
     unsigned char* Bs = As + kTileBytes;
-    stage_tile(As, g.A, g.lda, g.M, g.K, m0, kt * TBK, !g.transA, vecA);
-    stage_tile(Bs, g.B, g.ldb, g.N, g.K, n0, kt * TBK, g.transB != 0, vecB);
+    if (tma && threadIdx.x == 0) {
+      tc::mbar_expect_tx(&full[s], tx_bytes);
+      if (maps.tma_a) tc::tma_load_2d(As, &maps.a, kt * TBK, m0, &full[s]);
+      if (maps.tma_b) tc::tma_load_2d(Bs, &maps.b, kt * TBK, n0, &full[s]);
+    }
+    if (!maps.tma_a) stage_tile(As, g.A, g.lda, g.M, g.K, m0, kt * TBK, !g.transA, vecA);
+    if (!maps.tma_b) stage_tile(Bs, g.B, g.ldb, g.N, g.K, n0, kt * TBK, g.transB != 0, vecB);
     tc::fence_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) {
-      tc::fence_after_sync();
-      const uint32_t a0 = tc::smem_u32(As), b0 = tc::smem_u32(Bs);
+      if (tma && !tc::mbar_wait(&full[s], (uint32_t)(kt >> 1) & 1u)) {
+        ok = false;  // no MMA: the next wait on this stage gives up too, and every thread leaves
+      } else {
+        tc::fence_after_sync();
+        const uint32_t a0 = tc::smem_u32(As), b0 = tc::smem_u32(Bs);
 #pragma unroll
-      for (int k = 0; k < TBK / 16; ++k)
-        tc::mma_f16(tmem, tc::smem_desc(a0 + k * 256, 128, 1024, 0), tc::smem_desc(b0 + k * 256, 128, 1024, 0), idesc,
-                    (kt > 0 || k > 0) ? 1u : 0u);
-      tc::mma_commit(&bars[s]);
+        for (int k = 0; k < TBK / 16; ++k) {
+          // TMA tiles: rows 128 bytes apart (128-byte swizzle), slice k at +32 k bytes;
+          // staged tiles: core matrices (LBO 128, SBO 1024), slice k at +256 k bytes.
+          const uint64_t ad = maps.tma_a ? tc::smem_desc(a0 + k * 32, 16, 1024, 2)
+                                         : tc::smem_desc(a0 + k * 256, 128, 1024, 0);
+          const uint64_t bd = maps.tma_b ? tc::smem_desc(b0 + k * 32, 16, 1024, 2)
+                                         : tc::smem_desc(b0 + k * 256, 128, 1024, 0);
+          tc::mma_f16(tmem, ad, bd, idesc, (kt > 0 || k > 0) ? 1u : 0u);
+        }
+        tc::mma_commit(&bars[s]);
+      }
     }
   }
   if (ok && KT > 0 && !tc::mbar_wait(&bars[(KT - 1) & 1], (uint32_t)((KT - 1) >> 1) & 1u)) ok = false;
@@ -272,6 +301,51 @@ __global__ void logq_kernel(const float* __restrict__ z, const __nv_bfloat16* __
 
 }  // namespace
 
+namespace {
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the library does not
+// link the driver, so it loads on machines without one).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = []() -> EncodeTiledFn {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return (EncodeTiledFn)p;
+  }();
+  return fn;
+}
+
+// Tensor map of a K-major bf16 operand [rows][ld] (K innermost): boxes of 64 x 128 with
+// 128-byte swizzle, zero fill outside the operand.  False when TMA cannot load it (row
+// pitch not a multiple of 16 bytes, unaligned base, or no encoder).
+bool tma_operand(CUtensorMap* map, const __nv_bfloat16* ptr, int ld, int K, int rows) {
+  if (((uintptr_t)ptr & 15) != 0 || (ld % 8) != 0 || K <= 0 || rows <= 0) return false;
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)TBK, (cuuint32_t)TBM};
+  const cuuint32_t estr[2] = {1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)ptr, dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// TMA operand loads on (default) or off (every operand staged by the threads).
+bool g_gemm_tma = true;
+}  // namespace
+
+int gemm_set_tma(int on) {
+  g_gemm_tma = on != 0;
+  return RGS_OK;
+}
+
 int gemm_bf16(const GemmArgs& g, cudaStream_t s) {
   if (g.M <= 0 || g.N <= 0 || g.K <= 0 || !g.A || !g.B || (!g.C && !g.Cb)) return fail(RGS_ERR_ARG, "bad GEMM");
   static bool configured[64] = {false};
@@ -281,8 +355,13 @@ int gemm_bf16(const GemmArgs& g, cudaStream_t s) {
     RGS_CUDA_TRY(cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem));
     configured[device] = true;
   }
+  GemmMaps maps;
+  std::memset(&maps, 0, sizeof(maps));
+  // A is K-major unless transposed; B is K-major when transposed ([N][ldb]).
+  if (g_gemm_tma && !g.transA && tma_operand(&maps.a, g.A, g.lda, g.K, g.M)) maps.tma_a = 1;
+  if (g_gemm_tma && g.transB && tma_operand(&maps.b, g.B, g.ldb, g.K, g.N)) maps.tma_b = 1;
   dim3 grid((g.N + TBN - 1) / TBN, (g.M + TBM - 1) / TBM);
-  gemm_tc_kernel<<<grid, 128, kGemmSmem, s>>>(g);
+  gemm_tc_kernel<<<grid, 128, kGemmSmem, s>>>(g, maps);
   RGS_CUDA_TRY(cudaGetLastError());
   return RGS_OK;
 }

@@ -22,6 +22,8 @@ struct GemmArgs {
 };
 
 int gemm_bf16(const GemmArgs& g, cudaStream_t s);
+// TMA loads of the K-major aligned GEMM operands on (1, default) or off (0).
+int gemm_set_tma(int on);
 // Reads and clears the flag that a bounded tensor-core wait gave up (synchronous).
 int tensor_core_status(int* timed_out);
 int bce_grad(const float* z, const float* target, int count, float scale, __nv_bfloat16* dz, double* partial,

@@ -153,6 +153,32 @@ class MadeProposal:
                                                  _p(buf["z"]), self._stream()))
         return buf["x"], buf["logq"]
 
+    def sample_mixture(self, count, mix, seed=0, first=0):
+        """Samples of the defensive mixture q_mix = (1 - mix) q + mix 2^-n with log q_mix:
+        each row of a network sample is replaced, with probability `mix`, by uniform bits
+        (seeded host draws), and log q_mix of every row comes from one log-q pass.  Where
+        the network underestimates p, q_mix >= mix 2^-n bounds p / q_mix by 2^n p / mix,
+        so the exact envelope max p / q_mix stays near the bulk's ratio."""
+        if not 0.0 < mix < 1.0:
+            raise ValueError("mix must lie in (0, 1)")
+        x, _ = self.sample(count, seed, first)
+        rng = np.random.default_rng([int(seed) & (2 ** 63 - 1), int(first) & (2 ** 63 - 1), 0x6D6978])
+        repl = rng.random(count) < mix
+        if repl.any():
+            u = torch.from_numpy(rng.integers(0, 2, (int(repl.sum()), self.n)).astype(np.float32)).to(self.device)
+            idx = torch.from_numpy(np.flatnonzero(repl)).to(self.device)
+            x = x.clone()
+            x[idx] = u.to(torch.bfloat16)
+        lq = self.log_q(x)
+        return x, self.mixture_log_q(lq, mix)
+
+    def mixture_log_q(self, lq, mix):
+        """log q_mix = log((1 - mix) q + mix 2^-n) from log q (tensor or array)."""
+        lu = math.log(mix) - self.n * math.log(2.0)
+        if isinstance(lq, torch.Tensor):
+            return torch.logaddexp(lq + math.log1p(-mix), torch.full_like(lq, lu))
+        return np.logaddexp(np.asarray(lq) + math.log1p(-mix), lu)
+
     def log_q(self, x_bf16):
         x_bf16 = self._input(x_bf16)
         batch = int(x_bf16.shape[0])

