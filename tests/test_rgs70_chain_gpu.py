@@ -32,3 +32,35 @@ def test_rgs70_chain_samples_rescored(pkg, fixtures):
     assert np.max(np.abs(logp - np.log(p128))) < 1e-4
     # Distinct strings (collisions among 8 Born samples of a 70-qubit state are vanishingly rare).
     assert len({b.tobytes() for b in bits}) == 8
+
+
+def test_rgs70_searched_order_samples_are_born(pkg, fixtures):
+    """256 exact samples with this package's searched order (rank 29, fused pairs): the law
+    of 2^n p(x) over the samples matches the reference's 3,452 Born samples (two-sample KS
+    p > 1e-3), and the linear XEB lies within 4 standard errors of the reference's pooled
+    1.025; each sample's p(x) and log p(x) agree with its complex128 rescoring."""
+    import json
+    from pathlib import Path
+    from scipy import stats
+
+    golden = Path(__file__).resolve().parent / "golden"
+    born = json.loads((golden / "rgs70_born.json").read_text())["probability_c128"]
+    zref = np.concatenate([born["batch1"], born["batch2"]]) * 2.0 ** 70
+    order = json.loads((golden / "searched_orders.json").read_text())["rgs70"]["order"]
+    g = fixtures["rgs70/graph"]
+    u = fixtures["rgs70/measurement_unitaries"]
+    cs = pkg.ChainSampler(g, u, order, precision="c64", batch_tile=8)
+    assert cs.plan.rmax == 29 and len(cs.plan.pairs) > 0
+    bits, p, logp = cs.sample(256, seed=2029)
+    del cs
+    torch.cuda.empty_cache()
+    z = p * 2.0 ** 70
+    assert stats.ks_2samp(z, zref).pvalue > 1e-3
+    se = z.std(ddof=1) / np.sqrt(len(z))
+    assert abs(z.mean() - 1 - 1.025) < 4 * se
+    assert np.max(np.abs(logp - np.log(p))) < 1e-4
+    so = pkg.ScanOracle(g, u, fixtures["rgs70/scan_order"].tolist(), fp64=True, batch_tile=4)
+    p128 = so.probabilities(bits[:16])
+    del so
+    torch.cuda.empty_cache()
+    assert np.max(np.abs(p[:16] - p128) / p128) < 1e-4
