@@ -19,6 +19,15 @@
 #ifndef RGS_PAIR_LOADS
 #define RGS_PAIR_LOADS 8
 #endif
+// RGS_STREAM_HINTS: table rows are read once and written once per pass, so loads and
+// stores may carry the evict-first (streaming) cache hint.
+#ifdef RGS_STREAM_HINTS
+#define RGS_LD(p) __ldcs(p)
+#define RGS_ST(p, v) __stcs(p, v)
+#else
+#define RGS_LD(p) __ldg(p)
+#define RGS_ST(p, v) (*(p) = (v))
+#endif
 
 namespace rgs {
 
@@ -62,9 +71,9 @@ template <>
 struct Chunk<float, 2> {
   float4 v;
   __device__ __forceinline__ void load(const float* E, u64 chunk) {
-    v = __ldg(reinterpret_cast<const float4*>(E) + chunk);
+    v = RGS_LD(reinterpret_cast<const float4*>(E) + chunk);
   }
-  __device__ __forceinline__ void store(float* E, u64 chunk) const { reinterpret_cast<float4*>(E)[chunk] = v; }
+  __device__ __forceinline__ void store(float* E, u64 chunk) const { RGS_ST(reinterpret_cast<float4*>(E) + chunk, v); }
   __device__ __forceinline__ float re(int i) const { return i ? v.z : v.x; }
   __device__ __forceinline__ float im(int i) const { return i ? v.w : v.y; }
   __device__ __forceinline__ void set(int i, float r, float m) {
@@ -82,9 +91,9 @@ template <>
 struct Chunk<float, 1> {
   float2 v;
   __device__ __forceinline__ void load(const float* E, u64 chunk) {
-    v = __ldg(reinterpret_cast<const float2*>(E) + chunk);
+    v = RGS_LD(reinterpret_cast<const float2*>(E) + chunk);
   }
-  __device__ __forceinline__ void store(float* E, u64 chunk) const { reinterpret_cast<float2*>(E)[chunk] = v; }
+  __device__ __forceinline__ void store(float* E, u64 chunk) const { RGS_ST(reinterpret_cast<float2*>(E) + chunk, v); }
   __device__ __forceinline__ float re(int) const { return v.x; }
   __device__ __forceinline__ float im(int) const { return v.y; }
   __device__ __forceinline__ void set(int, float r, float m) { v = make_float2(r, m); }
@@ -94,9 +103,9 @@ template <>
 struct Chunk<double, 1> {
   double2 v;
   __device__ __forceinline__ void load(const double* E, u64 chunk) {
-    v = __ldg(reinterpret_cast<const double2*>(E) + chunk);
+    v = RGS_LD(reinterpret_cast<const double2*>(E) + chunk);
   }
-  __device__ __forceinline__ void store(double* E, u64 chunk) const { reinterpret_cast<double2*>(E)[chunk] = v; }
+  __device__ __forceinline__ void store(double* E, u64 chunk) const { RGS_ST(reinterpret_cast<double2*>(E) + chunk, v); }
   __device__ __forceinline__ double re(int) const { return v.x; }
   __device__ __forceinline__ double im(int) const { return v.y; }
   __device__ __forceinline__ void set(int, double r, double m) { v = make_double2(r, m); }
