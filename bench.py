@@ -34,6 +34,9 @@ BATCH = 65536
 ORDER_SEEDS = range(1000, 3048)
 TARGET_RANK = 22
 BITS_SEED = 1234
+# Exact sampling legs: complex64 tables with float32 arithmetic (the bulk), branch masses
+# and conditional normalisation summed in float64 (the chain sampler's Gram matrices).
+CHAIN_PRECISION = "c64f32"
 
 
 def build_instance(pkg):
@@ -653,7 +656,8 @@ def run_chain(args, rank, world, local_rank, emit=True):
     if world > 1 and not dist.is_initialized():
         dist.init_process_group("nccl", device_id=device)
     chain_tile = min(args.tile64 or 128, 128)
-    cs = pkg.ChainSampler(inst.g, inst.u, inst.order, device=device, precision="c64", batch_tile=chain_tile)
+    cs = pkg.ChainSampler(inst.g, inst.u, inst.order, device=device, precision=CHAIN_PRECISION,
+                          batch_tile=chain_tile)
     stream = torch.cuda.current_stream(device)
     outs = cs._outs(BATCH)
     seed = [1000 + rank]
@@ -689,7 +693,7 @@ def run_chain(args, rank, world, local_rank, emit=True):
     line = {"metric": "exact_born_samples_per_s (chain rule over the scan, n=40 3-regular)",
             "value": world * BATCH * args.steps / t, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded graph and gates, Philox uniforms)",
+            "vs_baseline": None, "dtype": "c64 (fp32 math, fp64 branch masses)", "data": "synthetic (seeded graph and gates, Philox uniforms)",
             "config": {"workload": f"n=40 random 3-regular, r_max {inst.rmax}, {BATCH} samples per GPU per step",
                        "instance": inst.name, "batch_tile": chain_tile},
             "roofline": {"bound": "hbm", "achieved": bytes_per * BATCH * args.steps / t / 1e9,
@@ -918,7 +922,7 @@ def run_rgs70(args, rank, world, local_rank):
         S = 16
         sampled = {}
         for name, sorder in (("reference_optimised", optimised), ("searched", searched)):
-            cs = pkg.ChainSampler(g, u, sorder, device=device, precision="c64", batch_tile=8)
+            cs = pkg.ChainSampler(g, u, sorder, device=device, precision=CHAIN_PRECISION, batch_tile=8)
             outs = cs._outs(S)
             seed = [70000 + 1000 * rank]
 
@@ -1001,7 +1005,8 @@ def full_scale(pkg, device, S, legs=("random_order", "searched_order"), rescore=
         tile = 1
         while tile < 128 and 2 * (2 * tile) * 8 * (1 << plan.rmax) <= 120 * 2 ** 30 and 2 * tile <= S:
             tile *= 2
-        cs = pkg.ChainSampler(inst.g, inst.u, order, device=device, precision="c64", batch_tile=tile, plan=plan)
+        cs = pkg.ChainSampler(inst.g, inst.u, order, device=device, precision=CHAIN_PRECISION, batch_tile=tile,
+                              plan=plan)
         cs.sample_device(min(S, tile), seed=1, check=True, stream=stream)  # warm-up
         outs = cs._outs(S)
         torch.cuda.synchronize(device)
@@ -1055,7 +1060,7 @@ def run_full(args, rank, world, local_rank):
     line = {"metric": "exact_born_samples_per_s (n=70 degree<=3, rank 30, chain rule, complex64)",
             "value": main["samples_per_s"], "unit": "samples/s", "n_gpus": world, "steps": 1, "warmup": 1,
             "ms_per_step": 1e3 * main["seconds"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "c64", "data": "synthetic (seeded graph, gates, Philox uniforms)",
+            "dtype": "c64 (fp32 math, fp64 branch masses)", "data": "synthetic (seeded graph, gates, Philox uniforms)",
             "config": {"workload": f"full scale: n=70 random degree<=3 graph, seeded random order with r_max "
                                    f"{main['rmax']}, {S} exact samples, 256 rescored in complex128",
                        "instance": inst.name},
@@ -1083,7 +1088,7 @@ def learned_comparison(pkg, device, samples, train_samples, epochs, order_policy
     plan = pkg.ScanPlan(n, pkg.edges_from_graph(inst.g), order)
     if plan.rmax > 28:
         raise SystemExit(f"instance rank {plan.rmax} above 28")
-    cs = pkg.ChainSampler(inst.g, inst.u, order, device=device, precision="c64", batch_tile=batch_tile)
+    cs = pkg.ChainSampler(inst.g, inst.u, order, device=device, precision=CHAIN_PRECISION, batch_tile=batch_tile)
     so = pkg.ScanOracle(inst.g, inst.u, order, device=device, precision="c64f32")
     so128 = pkg.ScanOracle(inst.g, inst.u, order, device=device, fp64=True)
     order_a = np.asarray(order)

@@ -14,13 +14,12 @@
 //                         log p(x_v | prefix), and the weights of the chosen branch
 //   scan step kernel    : the chosen branch, with the usual power-of-two renormalisation
 // so a sample costs one scan sweep plus one read of the tables of the other positions.
-// Fused pairs of the plan (positions j, j + 1; complex64 tables with float64 arithmetic
-// and complex128): x_j as above; then one pass over j's input forms j's outputs in
-// registers and accumulates the Gram matrix of position j + 1 (scan_pair_kernel, GRAM
-// mode, no stores) unless j + 1 is analytic; x_{j+1}; then the pair kernel writes the
-// output of j + 1.  The table between the two positions never reaches memory: per pair
-// 2 reads of j's input and 1 write instead of 1 read, 3 passes over the intermediate
-// table and 1 write.
+// Fused pairs of the plan (positions j, j + 1): x_j as above; then one pass over j's
+// input forms j's outputs in registers and accumulates the Gram matrix of position j + 1
+// (scan_pair_kernel, GRAM mode, no stores, float64 sums) unless j + 1 is analytic;
+// x_{j+1}; then the pair kernel writes the output of j + 1.  The table between the two
+// positions never reaches memory: per pair 2 reads of j's input and 1 write instead of 1
+// read, 3 passes over the intermediate table and 1 write.
 // The final table is the amplitude of the drawn string, returned like rgs_scan_amplitudes.
 #include <cuda_runtime.h>
 
@@ -41,6 +40,7 @@ namespace {
 
 constexpr int kMassBlocks = 296;   // 2 blocks (the occupancy of the Gram kernel) on each of 148 SMs
 constexpr int kChainMaxTile = 128;  // largest batch tile (complex64); complex128: 64
+constexpr int kDecideThreads = 128;  // threads of the per-item decision block
 
 // Gram matrix of one position per item, from one read of the table (no writes).  Every
 // output of the step is alpha f(0) + beta f(1) with f = U_v[x, :] s: in pair mode row c'
@@ -203,23 +203,24 @@ __global__ void chain_decide_kernel(const double* __restrict__ partial, int nblo
                                     long long first, const double* __restrict__ uniforms, int n, u64 seed,
                                     double4* __restrict__ Wj, double* __restrict__ logp, float* __restrict__ cond1,
                                     int* __restrict__ status) {
-  // One warp per item: lanes sum strided block partials, then a fixed shuffle tree.
-  const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (b >= Bt) return;
+  // One block per item: threads sum strided block partials, then a fixed shuffle tree
+  // per warp and the warps in order (deterministic).
+  __shared__ double wsum[kDecideThreads / 32][4];
+  const int b = blockIdx.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (b >= count) {
-    if (lane == 0) Wj[b] = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (threadIdx.x == 0) Wj[b] = make_double4(0.0, 0.0, 0.0, 0.0);
     return;
   }
   double g0 = 1.0, g1 = 1.0, g2 = 0.0, g3 = 0.0;
   if (!analytic) {
     g0 = g1 = 0.0;
-    for (int k = lane; k < nblocks; k += 32) {
-      const double* p = partial + ((size_t)k * Bt + b) * 4;
-      g0 += p[0];
-      g1 += p[1];
-      g2 += p[2];
-      g3 += p[3];
+    for (int k = threadIdx.x; k < nblocks; k += blockDim.x) {
+      const double4 p = *reinterpret_cast<const double4*>(partial + ((size_t)k * Bt + b) * 4);
+      g0 += p.x;
+      g1 += p.y;
+      g2 += p.z;
+      g3 += p.w;
     }
     for (int off = 16; off; off >>= 1) {
       g0 += __shfl_xor_sync(0xffffffffu, g0, off);
@@ -227,8 +228,24 @@ __global__ void chain_decide_kernel(const double* __restrict__ partial, int nblo
       g2 += __shfl_xor_sync(0xffffffffu, g2, off);
       g3 += __shfl_xor_sync(0xffffffffu, g3, off);
     }
+    if (lane == 0) {
+      wsum[wid][0] = g0;
+      wsum[wid][1] = g1;
+      wsum[wid][2] = g2;
+      wsum[wid][3] = g3;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      g0 = g1 = g2 = g3 = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        g0 += wsum[w][0];
+        g1 += wsum[w][1];
+        g2 += wsum[w][2];
+        g3 += wsum[w][3];
+      }
+    }
   }
-  if (lane) return;
+  if (threadIdx.x) return;
   const double m0 = branch_mass(U + (v * 2 + 0) * 2, g0, g1, g2, g3);
   const double m1 = branch_mass(U + (v * 2 + 1) * 2, g0, g1, g2, g3);
   const double tot = m0 + m1;
@@ -340,9 +357,8 @@ int chain_run(Plan& plan, const double* U, long long count, int mode_given, u64 
   int* status = (int*)(ws + L.off_status);
   const u64* tables = (const u64*)dc->tables;
   const double2* U2 = (const double2*)U;
-  // Fused pairs of positions (the plan's pairs) for complex64 tables with float64
-  // arithmetic and for complex128.
-  const bool fuse = (precision == RGS_PREC_C64 || precision == RGS_PREC_C128) && !plan.pair_at.empty();
+  // Fused pairs of positions (the plan's pairs), every precision.
+  const bool fuse = !plan.pair_at.empty();
   RGS_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), stream));
   for (long long first = 0; first < count; first += Bt) {
     const int cnt = (int)std::min<long long>(Bt, count - first);
@@ -359,7 +375,7 @@ int chain_run(Plan& plan, const double* U, long long count, int mode_given, u64 
                                          j == 0);
         if (e != cudaSuccess) return e;
       }
-      chain_decide_kernel<<<(Bt * 32 + 127) / 128, 128, 0, stream>>>(
+      chain_decide_kernel<<<Bt, kDecideThreads, 0, stream>>>(
           partial, L.mass_blocks, analytic, Bt, cnt, j, st.v, U2, mode_given, bits, first, uniforms, plan.n, seed,
           W + (size_t)j * Bt, out_logp, out_cond1, status);
       return cudaGetLastError();

@@ -416,7 +416,7 @@ cudaError_t scan_launch_pair_gram(int precision, int Bt, int blocks, const DevPa
   const dim3 grid((unsigned)blocks);
   if (precision == RGS_PREC_C128) return launch_pair_gram_c128(VE, grid, s, Ein, P, tables, WA, mp, lbt, partial);
   if (precision == RGS_PREC_C64) return launch_pair_gram_c64(VE, grid, s, Ein, P, tables, WA, mp, lbt, partial);
-  return cudaErrorInvalidValue;
+  return launch_pair_gram_f32(VE, grid, s, Ein, P, tables, WA, mp, lbt, partial);
 }
 
 namespace {

@@ -66,14 +66,16 @@ cudaError_t launch_pair_gram_c64(int VE, dim3 grid, cudaStream_t s, const void* 
 cudaError_t launch_pair_gram_c128(int VE, dim3 grid, cudaStream_t s, const void* Ein, const DevPair& P,
                                   const unsigned long long* tables, const double4* WA, const unsigned long long* mp,
                                   int lbt, double* partial);
+cudaError_t launch_pair_gram_f32(int VE, dim3 grid, cudaStream_t s, const void* Ein, const DevPair& P,
+                                 const unsigned long long* tables, const double4* WA, const unsigned long long* mp,
+                                 int lbt, double* partial);
 // One fused pair (positions P.j, P.j + 1) over one batch tile.
 cudaError_t scan_launch_pair(int precision, int Bt, int device, const DevPair& P, const void* Ein, void* Eout,
                              const unsigned long long* tables, const double4* WA, const double4* WB,
                              const unsigned long long* mp, unsigned long long* mA, unsigned long long* mc,
                              cudaStream_t s);
 // B's Gram partials of a fused pair over one batch tile: `blocks` blocks write
-// partial[blocks][Bt][4] (G00, G11, Re G01, Im G01 of B's branch masses); precisions
-// RGS_PREC_C64 and RGS_PREC_C128.
+// partial[blocks][Bt][4] (G00, G11, Re G01, Im G01 of B's branch masses, float64 sums).
 cudaError_t scan_launch_pair_gram(int precision, int Bt, int blocks, const DevPair& P, const void* Ein,
                                   const unsigned long long* tables, const double4* WA, const unsigned long long* mp,
                                   double* partial, cudaStream_t s);
