@@ -1159,6 +1159,73 @@ def learned_comparison(pkg, device, samples, train_samples, epochs, order_policy
                      "kl_estimate": float(np.mean(losses[-5:]) - floor)}}
 
 
+def run_wht(args, rank, world, local_rank):
+    """Config 2's WHT variants on their own: FP32 butterflies vs 16 x 16 Hadamard blocks on
+    the tensor cores over split-BF16 values, on a 2^m state (`--m`)."""
+    import torch
+    import __graft_entry__
+    pkg = __graft_entry__.package()
+    device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+    peaks_path = ROOT / "MEASURED_PEAKS.json"
+    peak = float(json.loads(peaks_path.read_text())["hbm_gbs"]) if peaks_path.exists() else 6650.0
+    res = wht_precision_leg(pkg, device, peak, m=args.m)
+    if rank == 0:
+        best = res["fp32"]
+        print(json.dumps({"metric": f"full WHT of a 2^{args.m} complex64 state (fp32 vs split-bf16 tensor cores)",
+                          "value": best["achieved_GBps"], "unit": "GB/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+                          "ms_per_step": best["ms"], "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "c64", "data": "synthetic (Gaussian state)",
+                          "config": {"workload": f"WHT on all {args.m} bits"}, "variants": res}), flush=True)
+
+
+def run_gemm(args, rank, world, local_rank):
+    """The proposal network's forward GEMM shape on the tcgen05 kernel: C[8192 x 512] =
+    A[8192 x 512] B[512 x 512]^T in BF16 with FP32 accumulation (both operands K-major,
+    TMA-loaded), 3 warm-up and 20 timed launches."""
+    import ctypes
+    import torch
+    import __graft_entry__
+    pkg = __graft_entry__.package()
+    device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+    M, N, K = 8192, 512, 512
+    a = torch.randn(M, K, device=device).to(torch.bfloat16)
+    b = torch.randn(N, K, device=device).to(torch.bfloat16)
+    c = torch.empty(M, N, device=device)
+    lib = pkg._lib.lib()
+    stream = torch.cuda.current_stream(device)
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+
+    def launch():
+        pkg._lib.check(lib.rgs_gemm_bf16(M, N, K, ptr(a), K, 0, ptr(b), K, 1, 1.0, None, 0, None, None, ptr(c),
+                                         None, N, ctypes.c_void_p(stream.cuda_stream)))
+    for _ in range(3):
+        launch()
+    torch.cuda.synchronize(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(20):
+        launch()
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    t = e0.elapsed_time(e1) / 20 / 1e3
+    ref = a[:256].float() @ b.float().T
+    err = float((c[:256] - ref).abs().max())
+    peaks_path = ROOT / "MEASURED_PEAKS.json"
+    peak = float(json.loads(peaks_path.read_text())["bf16_tflops"]) if peaks_path.exists() else 1590.0
+    tflops = 2 * M * N * K / t / 1e12
+    if rank == 0:
+        print(json.dumps({"metric": "tflops (tcgen05 bf16 GEMM, MADE forward shape 8192 x 512 x 512)",
+                          "value": tflops, "unit": "TFLOP/s", "n_gpus": 1, "steps": 20, "warmup": 3,
+                          "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "bf16 (fp32 accumulation)", "data": "synthetic (Gaussian operands)",
+                          "config": {"workload": "C = A B^T, M=8192 N=512 K=512, TMA-loaded K-major operands"},
+                          "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s",
+                                       "frac": tflops / peak},
+                          "max_abs_err_vs_torch_fp32": err}), flush=True)
+
+
 def run_learned(args, rank, world, local_rank):
     """Learned proposal workload (config 4) at full size: 2^16 training samples, `--samples`
     accepted samples; `--order random` keeps the seeded random order (rank 25)."""
@@ -1191,7 +1258,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the other configurations' legs of the default line (profiling runs)")
-    ap.add_argument("--workload", choices=["amplitudes", "fourier", "chain", "learned", "batched", "rgs70", "full"], default="amplitudes")
+    ap.add_argument("--workload", choices=["amplitudes", "fourier", "chain", "learned", "batched", "rgs70", "full",
+                                           "wht", "gemm"], default="amplitudes")
     ap.add_argument("--samples", type=int, default=4096, help="learned: accepted samples; full: exact samples")
     ap.add_argument("--epochs", type=int, default=8, help="training epochs of the learned workload")
     ap.add_argument("--order", choices=["searched", "random"], default="searched",
@@ -1223,6 +1291,10 @@ def main():
         run_rgs70(args, rank, world, local_rank)
     elif args.workload == "full":
         run_full(args, rank, world, local_rank)
+    elif args.workload == "wht":
+        run_wht(args, rank, world, local_rank)
+    elif args.workload == "gemm":
+        run_gemm(args, rank, world, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
 
