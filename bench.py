@@ -597,9 +597,10 @@ def run_fourier(args, rank, world, local_rank):
     torch.cuda.set_device(device)
     m = args.m
     g, u, A, B = fourier_instance(pkg, m)
+    L = pkg._lib.lib()
+    pkg._lib.check(L.rgs_fourier_set_register_schedule(1 if args.pass_kernel == "registers" else 0))
     s = pkg.ConditionalSampler(g, u, A, B, [local_rank])
     variant, tune_ms = s.tune()
-    L = pkg._lib.lib()
     stream = torch.cuda.current_stream(device)
     rng = np.random.default_rng(99 + rank)
 
@@ -635,7 +636,7 @@ def run_fourier(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded dense graph)",
             "config": {"workload": f"conditional sampler, dense graph n={2 * m}, full-rank balanced cut m={m}",
-                       "passes": s.passes, "specialized": s.specialized,
+                       "passes": s.passes, "specialized": s.specialized, "pass_kernel": args.pass_kernel,
                        "tuned_variant": {"chosen": variant, "ms_per_compute": tune_ms,
                                          "variants": "3 or 4 resident blocks per SM"}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -1265,6 +1266,9 @@ def main():
     ap.add_argument("--order", choices=["searched", "random"], default="searched",
                     help="scan order of the learned workload's n=56 instance")
     ap.add_argument("--m", type=int, default=30, help="conditional qubits of the fourier workload")
+    ap.add_argument("--pass-kernel", choices=["registers", "rounds"], default="registers",
+                    help="fourier workload: register-first pass kernel (default) or one shared-memory "
+                         "round per four axes")
     ap.add_argument("--tile64", type=int, default=None, help="complex64 batch tile (default: autotuned)")
     ap.add_argument("--bulk", choices=["c64f32", "c64"], default="c64f32",
                     help="complex64 bulk arithmetic: float32 (default) or float64")

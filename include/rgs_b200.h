@@ -250,6 +250,12 @@ int rgs_fourier_compute(rgs_fourier* plan, uint64_t outB, void* state, void* wor
  * synchronises. */
 int rgs_fourier_tune(rgs_fourier* plan, void* state, void* workspace, size_t workspace_bytes, void* stream,
                      int32_t* variant, float* ms);
+/* Pass kernel of the 12-bit tiles: register-first schedule (1, default: axes applied in
+ * registers at the load and before the store, the rest in up to three shared-memory
+ * rounds) or one shared-memory round per four axes (0).  Both apply the same 2x2
+ * operations per axis, in a different order across axes (FP32 results agree to rounding).
+ * Exists for tests and measurements.  Process-wide. */
+int rgs_fourier_set_register_schedule(int32_t on);
 /* The reference base pipeline (distributed_sampler.py:126-144): product init over b,
  * WHT, index map with q_A phase into `scratch`, products; result in `scratch`. */
 int rgs_fourier_compute_permute(rgs_fourier* plan, uint64_t outB, void* state, void* scratch, void* workspace,

@@ -31,9 +31,11 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <atomic>
 #include <mutex>
 
 #include "common.hpp"
+#include "f32x2.cuh"
 #include "fourier.cuh"
 
 namespace rgs {
@@ -61,6 +63,19 @@ enum InitKind : int { INIT_LOAD = 0, INIT_COV_GENERIC = 1, INIT_COV_SPECIAL = 2,
 // in `base`, b(base ^ f) = b(base) ^ mlo[f & 63] ^ mhi[f >> 6] and
 // q(base ^ f) = q(base) ^ qtab[f] ^ parity(L & f), L_a = parity(qsym[global(a)] & base)
 // (q is a polynomial of degree 2, so q(x ^ y) = q(x) ^ q(y) ^ x^T (Q + Q^T) y).
+// Register-first schedule of a 12-bit tile (see fourier_sched_kernel): the tile axes
+// applied in registers after the load (layout L0), in up to three shared-memory rounds
+// (window [rw0, rw0 + 4)), and in registers before the store (layout L0 or L1).
+struct PassSched {
+  unsigned ld_w, ld_u;            // WHT / product axes at the load stage
+  int nr;                         // shared-memory rounds
+  int rw0[3];
+  unsigned rw[3], ru[3];
+  int fin_l1;                     // final layout L1 (else L0)
+  unsigned fw, fu;
+  int phase_at;                   // stage of the phase: 0 load, 1..nr rounds, nr + 1 final, -1 none
+};
+
 struct PassParams {
   float2* v;
   int m, c, K, q;                 // tile = c low bits + K target bits at q
@@ -74,7 +89,7 @@ struct PassParams {
   const double2* wspec;           // [(m+1)^2] popcount weights
   u64 outmask;
   const double2* u;               // [m][2][2] complex128 per global bit
-  const float2* rot;              // [m] (c, s): products are real rotations (Euler-factorised path)
+  const float2* rot;              // [m] (k, form): scaled real rotations (Euler-factorised path)
   const float2* dg;               // chunk tables of the diagonal applied with the q_A phase, or null
   const float2* dh;               // chunk tables of the diagonal applied after the products, or null
   const float2* rg;               // [m] per-bit ratios d_j(1) / d_j(0) of the dg diagonal
@@ -94,6 +109,8 @@ struct PassParams {
   u64 tile0;
   u64 ntiles;                     // tiles of this launch (0: every tile of the index space)
   int store_top;
+  int sched;                      // 1: register-first schedule below (fourier_sched_kernel)
+  PassSched s;
 };
 
 // Padded shared-memory layout: one spare slot per 16 elements, so the 16 threads of a
@@ -197,6 +214,25 @@ __device__ __forceinline__ float2 window_factor(const float2 (*wt)[16], int f) {
   return cmulf(cmulf(wt[0][f & 15], wt[1][(f >> 4) & 15]), wt[2][(f >> 8) & 15]);
 }
 
+// The elements of thread t are f = 2 t + 2 k nt + e (k < 8, e < 2).  With nt >= 128 their
+// low 8 bits are those of 2 t + e for every k, so the first two windows' factor is one
+// value per e for the whole loop (lo[e]) and each element needs the third window only.
+struct WindowSplit {
+  bool on;
+  float2 lo[2];
+};
+__device__ __forceinline__ WindowSplit window_split(const float2 (*wt)[16], int nt) {
+  WindowSplit w;
+  w.on = nt >= 128;
+  const int f = (2 * threadIdx.x) & 255;
+#pragma unroll
+  for (int e = 0; e < 2; ++e) w.lo[e] = cmulf(wt[0][(f + e) & 15], wt[1][((f + e) >> 4) & 15]);
+  return w;
+}
+__device__ __forceinline__ float2 window_factor(const float2 (*wt)[16], const WindowSplit& w, int f, int e) {
+  return w.on ? cmulf(w.lo[e], wt[2][(f >> 8) & 15]) : window_factor(wt, f + e);
+}
+
 // Loads a pass's tables into shared memory and evaluates the tile constants: b(base)
 // (when `map`), q(base) and the 12-bit linear mask L of the cross term.
 __device__ __forceinline__ void tile_tables_setup(const PassParams& P, const TileTables* tt, const u64* lut,
@@ -262,10 +298,17 @@ __device__ __forceinline__ void apply_u(float2& x, float2& y, const float2 (&u)[
   y = ny;
 }
 
-// Real rotation [[c, -s], [s, c]] on a pair of complex values: 4 FMUL + 4 FFMA.
-__device__ __forceinline__ void apply_rot(float2& x, float2& y, float c, float s) {
-  const float2 nx = make_float2(fmaf(c, x.x, -s * y.x), fmaf(c, x.y, -s * y.y));
-  const float2 ny = make_float2(fmaf(s, x.x, c * y.x), fmaf(s, x.y, c * y.y));
+// Scaled real rotation on a pair of complex values, one packed FMA per output (the
+// rotation's scale and sign are folded into the diagonal applied after the products):
+//   form 0: [[1, -k], [k, 1]]   (k = s / c, |c| >= |s|)
+//   form 1: [[-k, 1], [1, k]]   (k = c / s, |s| > |c|)
+__device__ __forceinline__ void apply_rot0(float2& x, float2& y, float2 k, float2 nk) {
+  const float2 nx = f2fma(nk, y, x), ny = f2fma(k, x, y);
+  x = nx;
+  y = ny;
+}
+__device__ __forceinline__ void apply_rot1(float2& x, float2& y, float2 k, float2 nk) {
+  const float2 nx = f2fma(nk, x, y), ny = f2fma(k, y, x);
   x = nx;
   y = ny;
 }
@@ -290,15 +333,20 @@ __device__ void tile_round(float2* sm, const PassParams& P, int w0, unsigned mas
       for (int i = 0; i < 16; ++i) {
         if (i & (1 << a)) continue;
         const float2 x = r[i], y = r[i | (1 << a)];
-        r[i] = make_float2(x.x + y.x, x.y + y.y);
-        r[i | (1 << a)] = make_float2(x.x - y.x, x.y - y.y);
+        r[i] = f2add(x, y);
+        r[i | (1 << a)] = f2sub(x, y);
       }
     } else if (P.rot) {
-      const float2 cs = __ldg(P.rot + local_to_global_bit(P, w0 + a));
+      const float2 kf = __ldg(P.rot + local_to_global_bit(P, w0 + a));
+      const float2 k = make_float2(kf.x, kf.x), nk = make_float2(-kf.x, -kf.x);
+      if (kf.y == 0.f) {
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        if (i & (1 << a)) continue;
-        apply_rot(r[i], r[i | (1 << a)], cs.x, cs.y);
+        for (int i = 0; i < 16; ++i)
+          if (!(i & (1 << a))) apply_rot0(r[i], r[i | (1 << a)], k, nk);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+          if (!(i & (1 << a))) apply_rot1(r[i], r[i | (1 << a)], k, nk);
       }
     } else {
       const double2* u4 = P.u + 4 * local_to_global_bit(P, w0 + a);
@@ -362,13 +410,19 @@ __global__ void __launch_bounds__(256, MINB) fourier_pass_kernel(const __grid_co
     const u64 b0 = s_b0;
     const int q0 = s_q0;
     const unsigned lm = s_lm;
+    // Elements f = 2 t + 2 k nt + e: with nt >= 32 the low 6 bits of f are those of 2 t + e
+    // for every k, so b0 ^ mlo[f & 63] is one value per e for the whole loop.
+    const bool lo_const = nt >= 32;
+    const int t2 = 2 * (int)threadIdx.x;
+    const u64 blo[2] = {b0 ^ s_tt.mlo[t2 & 63], b0 ^ s_tt.mlo[(t2 + 1) & 63]};
 #pragma unroll 2
     for (int k = 0; k < 8; ++k) {
-      const int f0 = 2 * (threadIdx.x + k * nt);
+      const int f0 = t2 + 2 * k * nt;
+      const u64 bhi = s_tt.mhi[(f0 >> 6) & 63];
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int f = f0 + e;
-        const u64 b = b0 ^ s_tt.mlo[f & 63] ^ s_tt.mhi[(f >> 6) & 63];
+        const u64 b = (lo_const ? blo[e] : b0 ^ s_tt.mlo[f & 63]) ^ bhi;
         const float2 w = __ldg(P.wspecf + __popcll(b) * (P.m + 1) + __popcll(b & P.outmask));
         sm[pad(f)] = tile_q(s_tt, q0, lm, f) ? make_float2(-w.x, -w.y) : w;
       }
@@ -409,13 +463,14 @@ __global__ void __launch_bounds__(256, MINB) fourier_pass_kernel(const __grid_co
     __syncthreads();
     const int q0 = s_q0;
     const unsigned lm = s_lm;
+    const WindowSplit ws = window_split(wt, nt);
     for (int k = 0; k < 8; ++k) {
       const int f0 = 2 * (threadIdx.x + k * nt);
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int f = f0 + e;
         float2 x = sm[pad(f)];
-        if (P.dg) x = cmulf(x, window_factor(wt, f));
+        if (P.dg) x = cmulf(x, window_factor(wt, ws, f0, e));
         if (tile_q(s_tt, q0, lm, f)) x = make_float2(-x.x, -x.y);
         sm[pad(f)] = x;
       }
@@ -444,23 +499,27 @@ __global__ void __launch_bounds__(256, MINB) fourier_pass_kernel(const __grid_co
     window_tables(wt, P, P.dh, P.rh, base, TB);
   }
   __syncthreads();
-  float mass = 0.f;  // 16 elements per thread: float partial, then float64 across threads
+  const WindowSplit ws = window_split(wt, nt);
+  double mass = 0.0;  // per element pair: a float sum of four squares, then float64
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const int f = 2 * (threadIdx.x + k * nt);
     const u64 g = tile_global(P, tile, f);
     float2 a = sm[pad(f)], b = sm[pad(f + 1)];
     if (P.dh) {
-      a = cmulf(a, window_factor(wt, f));
-      b = cmulf(b, window_factor(wt, f + 1));
+      a = cmulf(a, window_factor(wt, ws, f, 0));
+      b = cmulf(b, window_factor(wt, ws, f, 1));
     }
     if (P.store && (P.store_top < 0 || (int)((g >> (P.m - 1)) & 1ull) == P.store_top))
       *reinterpret_cast<float4*>(P.v + (g & P.amask)) = make_float4(a.x, a.y, b.x, b.y);
-    if (P.masses) mass = fmaf(a.x, a.x, fmaf(a.y, a.y, fmaf(b.x, b.x, fmaf(b.y, b.y, mass))));
+    if (P.masses) {
+      const float2 q = f2fma(b, b, make_float2(a.x * a.x, a.y * a.y));
+      mass += (double)(q.x + q.y);
+    }
   }
   if (P.masses) {
     __shared__ double red[32];
-    double m2 = (double)mass;
+    double m2 = mass;
     for (int off = 16; off; off >>= 1) m2 += __shfl_xor_sync(0xffffffffu, m2, off);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m2;
     __syncthreads();
@@ -468,6 +527,271 @@ __global__ void __launch_bounds__(256, MINB) fourier_pass_kernel(const __grid_co
       double s = 0.0;
       for (int w = 0; w < (nt + 31) / 32; ++w) s += red[w];
       P.masses[tile - P.tile0] = s;
+    }
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Register-first passes (12-bit tiles, 256 threads).  Thread t holds 16 elements of the
+// tile in registers (index i = 2 k + e) in one of three arrangements:
+//   L0    : f = e + 2 t + 512 k                        axes 0, 9, 10, 11
+//   L1    : f = e + 2 (t & 31) + 64 k + 512 (t >> 5)   axes 0, 6, 7, 8
+//   round : f = f0(t) | (i << w0)                      axes w0 .. w0 + 3
+// L0 and L1 keep the lanes of a warp on axes 1..5, so global loads and stores stay
+// 16-byte accesses filling whole 32-byte sectors; every arrangement gives the 16 lanes
+// of a half-warp distinct 8-byte bank pairs in the padded layout.  The host schedule
+// (PassSched) applies every axis once -- at the load (L0), in a shared-memory round, or
+// before the store (L0 or L1) -- with all WHT axes before the phase and all products
+// after it.  Against one shared-memory round per four axes this saves up to two
+// exchanges per element and pass (four in the middle pass).
+
+__device__ __forceinline__ void reg_wht(float2 (&r)[16], const int (&ax)[4], unsigned wm) {
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    if (!((wm >> ax[a]) & 1u)) continue;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      if (i & (1 << a)) continue;
+      const float2 x = r[i], y = r[i | (1 << a)];
+      r[i] = f2add(x, y);
+      r[i | (1 << a)] = f2sub(x, y);
+    }
+  }
+}
+
+__device__ __forceinline__ void reg_prod(float2 (&r)[16], const PassParams& P, const int (&ax)[4], unsigned um) {
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    if (!((um >> ax[a]) & 1u)) continue;
+    const int gb = local_to_global_bit(P, ax[a]);
+    if (P.rot) {
+      const float2 kf = __ldg(P.rot + gb);
+      const float2 k = make_float2(kf.x, kf.x), nk = make_float2(-kf.x, -kf.x);
+      if (kf.y == 0.f) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+          if (!(i & (1 << a))) apply_rot0(r[i], r[i | (1 << a)], k, nk);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+          if (!(i & (1 << a))) apply_rot1(r[i], r[i | (1 << a)], k, nk);
+      }
+    } else {
+      const double2* u4 = P.u + 4 * gb;
+      float2 uu[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const double2 d = __ldg(u4 + e);
+        uu[e] = make_float2((float)d.x, (float)d.y);
+      }
+#pragma unroll
+      for (int i = 0; i < 16; ++i)
+        if (!(i & (1 << a))) apply_u(r[i], r[i | (1 << a)], uu);
+    }
+  }
+}
+
+// q_A phase (pass tables) times the diagonal dg, on the registers; fof(i) = tile index.
+template <class F>
+__device__ __forceinline__ void reg_phase(float2 (&r)[16], const PassParams& P, const float2 (*wt)[16],
+                                          const TileTables& st, int q0, unsigned lm, F fof) {
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const int f = fof(i);
+    float2 x = r[i];
+    if (P.dg) x = cmulf(x, window_factor(wt, f));
+    if (tile_q(st, q0, lm, f)) x = make_float2(-x.x, -x.y);
+    r[i] = x;
+  }
+}
+
+template <int W0>
+__device__ __forceinline__ int round_f0(int t) {
+  return (t & ((1 << W0) - 1)) | ((t >> W0) << (W0 + 4));
+}
+
+template <int W0, bool STORE>
+__device__ __forceinline__ void round_io(float2* sm, float2 (&r)[16]) {
+  float2* b = sm + pad(round_f0<W0>(threadIdx.x));
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    if (STORE)
+      b[pad(i << W0)] = r[i];
+    else
+      r[i] = b[pad(i << W0)];
+  }
+}
+
+template <bool STORE>
+__device__ __forceinline__ void round_io_at(float2* sm, float2 (&r)[16], int w0) {
+  switch (w0) {
+    case 0: round_io<0, STORE>(sm, r); break;
+    case 1: round_io<1, STORE>(sm, r); break;
+    case 2: round_io<2, STORE>(sm, r); break;
+    case 3: round_io<3, STORE>(sm, r); break;
+    case 4: round_io<4, STORE>(sm, r); break;
+    case 5: round_io<5, STORE>(sm, r); break;
+    case 6: round_io<6, STORE>(sm, r); break;
+    case 7: round_io<7, STORE>(sm, r); break;
+    default: round_io<8, STORE>(sm, r); break;
+  }
+}
+
+__device__ __forceinline__ int round_f0(int t, int w0) {
+  return (t & ((1 << w0) - 1)) | ((t >> w0) << (w0 + 4));
+}
+
+// Tile index of register i in layout L0 / L1 (t = thread).
+__device__ __forceinline__ int lay_f(int l1, int t, int i) {
+  const int e = i & 1, k = i >> 1;
+  return l1 ? e + 2 * (t & 31) + 64 * k + 512 * (t >> 5) : e + 2 * t + 512 * k;
+}
+
+// Global offset of a tile bit, and the addresses of a layout: g(k) = g0 + sum of the
+// offsets of k's bits (tile_global is a sum over the bits of f).
+__device__ __forceinline__ u64 gbit(const PassParams& P, int b) {
+  return b < P.c ? (1ull << b) : (1ull << (P.q + b - P.c));
+}
+struct LayAddr {
+  u64 g0, d[3];
+};
+__device__ __forceinline__ LayAddr lay_addr(const PassParams& P, u64 tile, int l1) {
+  const int t = threadIdx.x;
+  LayAddr A;
+  A.g0 = tile_global(P, tile, lay_f(l1, t, 0));
+  const int kb = l1 ? 6 : 9;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) A.d[j] = gbit(P, kb + j);
+  return A;
+}
+__device__ __forceinline__ u64 lay_g(const LayAddr& A, int k) {
+  return A.g0 + ((k & 1) ? A.d[0] : 0ull) + ((k & 2) ? A.d[1] : 0ull) + ((k & 4) ? A.d[2] : 0ull);
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) fourier_sched_kernel(const __grid_constant__ PassParams P) {
+  extern __shared__ float2 sm[];
+  __shared__ float2 wt[3][16];  // window tables of the pass's diagonal (dg or dh)
+  __shared__ TileTables s_tt;   // init or q_A pass tables
+  __shared__ u64 s_b0;
+  __shared__ int s_q0;
+  __shared__ unsigned s_lm;
+  const PassSched& S = P.s;
+  const int t = threadIdx.x;
+  const u64 tile = blockIdx.x + P.tile0;
+  const u64 base = tile_global(P, tile, 0);
+  const bool init_tab = P.init == INIT_COV_SPECIAL && P.tt_init;
+  if (init_tab)
+    tile_tables_setup(P, P.tt_init, P.lut_z, P.qsym_z, base, kTileBits, true, s_tt, s_b0, s_q0, s_lm);
+  else if (P.phase)
+    tile_tables_setup(P, P.tt_phase, P.lut_a, P.qsym_a, base, kTileBits, false, s_tt, s_b0, s_q0, s_lm);
+  if (P.dg)
+    window_tables(wt, P, P.dg, P.rg, base, kTileBits);
+  else if (P.dh)
+    window_tables(wt, P, P.dh, P.rh, base, kTileBits);
+  __syncthreads();
+  const int q0 = s_q0;
+  const unsigned lm = s_lm;
+  float2 r[16];
+  const LayAddr A0 = lay_addr(P, tile, 0);
+  // Load stage (L0): init computed in registers, or the state loaded.
+  if (init_tab) {
+    const u64 b0 = s_b0;
+    const u64 blo[2] = {b0 ^ s_tt.mlo[(2 * t) & 63], b0 ^ s_tt.mlo[(2 * t + 1) & 63]};
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const u64 bhi = s_tt.mhi[((2 * t + 512 * k) >> 6) & 63];
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int f = lay_f(0, t, 2 * k + e);
+        const u64 b = blo[e] ^ bhi;
+        const float2 w = __ldg(P.wspecf + __popcll(b) * (P.m + 1) + __popcll(b & P.outmask));
+        r[2 * k + e] = tile_q(s_tt, q0, lm, f) ? make_float2(-w.x, -w.y) : w;
+      }
+    }
+  } else if (P.init) {
+    const u64 varying = ((1ull << P.c) - 1ull) | (((1ull << P.K) - 1ull) << P.q);
+    TileLut tl;
+    tile_lut(P.lut_z, P.chunks, base, varying, tl);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const u64 g = lay_g(A0, k);
+      r[2 * k] = init_value(P, tl, g);
+      r[2 * k + 1] = init_value(P, tl, g + 1);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const float4 x = *reinterpret_cast<const float4*>(P.v + (lay_g(A0, k) & P.amask));
+      r[2 * k] = make_float2(x.x, x.y);
+      r[2 * k + 1] = make_float2(x.z, x.w);
+    }
+  }
+  const int ax0[4] = {0, 9, 10, 11};
+  reg_wht(r, ax0, S.ld_w);
+  if (P.phase && S.phase_at == 0) reg_phase(r, P, wt, s_tt, q0, lm, [&](int i) { return lay_f(0, t, i); });
+  reg_prod(r, P, ax0, S.ld_u);
+  const int fl = S.fin_l1;
+  if (S.nr > 0 || fl) {
+    float2* b0p = sm + pad(2 * t);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) b0p[(i & 1) + 544 * (i >> 1)] = r[i];
+    for (int j = 0; j < S.nr; ++j) {
+      __syncthreads();
+      const int w0 = S.rw0[j];
+      round_io_at<false>(sm, r, w0);
+      const int ax[4] = {w0, w0 + 1, w0 + 2, w0 + 3};
+      reg_wht(r, ax, S.rw[j]);
+      if (P.phase && S.phase_at == j + 1) {
+        const int f0 = round_f0(t, w0);
+        reg_phase(r, P, wt, s_tt, q0, lm, [&](int i) { return f0 | (i << w0); });
+      }
+      reg_prod(r, P, ax, S.ru[j]);
+      round_io_at<true>(sm, r, w0);
+    }
+    __syncthreads();
+    float2* bf = sm + pad(lay_f(fl, t, 0));
+#pragma unroll
+    for (int i = 0; i < 16; ++i) r[i] = bf[(i & 1) + (fl ? 68 : 544) * (i >> 1)];
+  }
+  const int axf[4] = {0, fl ? 6 : 9, fl ? 7 : 10, fl ? 8 : 11};
+  reg_wht(r, axf, S.fw);
+  if (P.phase && S.phase_at == S.nr + 1) reg_phase(r, P, wt, s_tt, q0, lm, [&](int i) { return lay_f(fl, t, i); });
+  reg_prod(r, P, axf, S.fu);
+  // Diagonal after the products (final layout L0 only), masses, store.
+  if (P.dh) {
+    const WindowSplit ws = window_split(wt, 256);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int f = lay_f(0, t, 2 * k);
+      r[2 * k] = cmulf(r[2 * k], window_factor(wt, ws, f, 0));
+      r[2 * k + 1] = cmulf(r[2 * k + 1], window_factor(wt, ws, f, 1));
+    }
+  }
+  const LayAddr Af = lay_addr(P, tile, fl);  // recomputed: A0 is not kept live across the rounds
+  double mass = 0.0;  // per element pair: a float sum of four squares, then float64
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const u64 g = lay_g(Af, k);
+    const float2 a = r[2 * k], b = r[2 * k + 1];
+    if (P.store && (P.store_top < 0 || (int)((g >> (P.m - 1)) & 1ull) == P.store_top))
+      *reinterpret_cast<float4*>(P.v + (g & P.amask)) = make_float4(a.x, a.y, b.x, b.y);
+    if (P.masses) {
+      const float2 q = f2fma(b, b, make_float2(a.x * a.x, a.y * a.y));
+      mass += (double)(q.x + q.y);
+    }
+  }
+  if (P.masses) {
+    __shared__ double red[8];
+    double m2 = mass;
+    for (int off = 16; off; off >>= 1) m2 += __shfl_xor_sync(0xffffffffu, m2, off);
+    if ((t & 31) == 0) red[t >> 5] = m2;
+    __syncthreads();
+    if (t == 0) {
+      double sum = 0.0;
+      for (int w = 0; w < 8; ++w) sum += red[w];
+      P.masses[tile - P.tile0] = sum;
     }
   }
 }
@@ -672,6 +996,7 @@ __global__ void __launch_bounds__(1024) shard_mass_kernel(const double* __restri
 
 // ------------------------------------------------------------------------------------- host
 std::mutex g_fourier_mutex;
+std::atomic<bool> g_fourier_legacy{false};  // true: every pass on fourier_pass_kernel
 
 template <int MINB>
 int set_smem_attr() {
@@ -680,23 +1005,94 @@ int set_smem_attr() {
   RGS_CUDA_TRY(cudaGetDevice(&device));
   std::lock_guard<std::mutex> lock(g_fourier_mutex);
   if (device >= 0 && device < 64 && done[device]) return RGS_OK;
-  RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_pass_kernel<MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    ((1 << kTileBits) + (1 << (kTileBits - 4))) * (int)sizeof(float2)));
+  const int bytes = ((1 << kTileBits) + (1 << (kTileBits - 4))) * (int)sizeof(float2);
+  RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_pass_kernel<MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_sched_kernel<MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   if (device >= 0 && device < 64) done[device] = true;
   return RGS_OK;
 }
 
-int launch_pass(const PassParams& P, cudaStream_t s) {
-  const int TB = P.c + P.K;
+// One stage sequence of the register-first kernel for a given round count and final
+// layout: every axis goes to the earliest stage that holds it, the phase (or the
+// WHT -> products boundary) to the stage where the last WHT axis is done.
+bool simulate_sched(unsigned W, unsigned U, bool phase, int n, const int* w0, int fl, PassSched& T) {
+  const unsigned R0 = 1u | (7u << 9), R1 = 1u | (7u << 6);
+  T = PassSched{};
+  bool pending = W != 0 || phase;
+  unsigned Wr = W, Ur = U;
+  T.phase_at = -1;
+  T.ld_w = Wr & R0;
+  Wr &= ~R0;
+  if (pending && !Wr) {
+    T.phase_at = 0;
+    pending = false;
+  }
+  T.ld_u = pending ? 0u : (Ur & R0);
+  Ur &= ~T.ld_u;
+  T.nr = n;
+  for (int j = 0; j < n; ++j) {
+    const unsigned win = 15u << w0[j];
+    T.rw0[j] = w0[j];
+    T.rw[j] = Wr & win;
+    Wr &= ~T.rw[j];
+    if (pending && !Wr) {
+      T.phase_at = j + 1;
+      pending = false;
+    }
+    T.ru[j] = pending ? 0u : (Ur & win);
+    Ur &= ~T.ru[j];
+  }
+  const unsigned Rf = fl ? R1 : R0;
+  if (Wr & ~Rf) return false;
+  T.fw = Wr;
+  if (pending) T.phase_at = n + 1;
+  if (Ur & ~Rf) return false;
+  T.fu = Ur;
+  T.fin_l1 = fl;
+  return true;
+}
+
+// Fewest shared-memory rounds (windows w0 in 0..8, all conflict-free in the padded
+// layout), final layout L0 preferred; false when three rounds do not suffice.
+bool plan_sched(const PassParams& P, PassSched& S) {
+  const bool phase = P.phase != 0;
+  for (int n = 0; n <= 3; ++n) {
+    int count = 1;
+    for (int j = 0; j < n; ++j) count *= 9;
+    for (int fl = 0; fl < 2; ++fl) {
+      if (fl && P.dh) continue;  // the diagonal after the products uses layout L0
+      for (int code = 0; code < count; ++code) {
+        int w0[3] = {0, 0, 0};
+        for (int j = 0, c = code; j < n; ++j, c /= 9) w0[j] = c % 9;
+        if (simulate_sched(P.wht_mask, P.u_mask, phase, n, w0, fl, S)) return true;
+      }
+    }
+  }
+  return false;
+}
+
+int launch_pass(const PassParams& Pin, cudaStream_t s) {
+  const int TB = Pin.c + Pin.K;
   if (TB < 4 || TB > kTileBits) return fail(RGS_ERR_UNSUPPORTED, "tile must span 4..13 bits");
-  const u64 tiles = P.ntiles ? P.ntiles : (1ull << (P.m - TB));
+  const u64 tiles = Pin.ntiles ? Pin.ntiles : (1ull << (Pin.m - TB));
   const size_t smem = ((1 << TB) + (1 << (TB - 4))) * sizeof(float2);
-  int rc = P.variant ? set_smem_attr<4>() : set_smem_attr<3>();
+  int rc = Pin.variant ? set_smem_attr<4>() : set_smem_attr<3>();
   if (rc) return rc;
-  if (P.variant)
+  PassParams P = Pin;
+  // The register-first kernel: 12-bit tiles, the phase from pass tables, at most one
+  // diagonal and not both the init and the phase.
+  P.sched = TB == kTileBits && !(P.init && P.phase) && !(P.phase && !P.tt_phase) && !(P.dg && P.dh) &&
+            !g_fourier_legacy && plan_sched(P, P.s);
+  if (P.sched) {
+    if (P.variant)
+      fourier_sched_kernel<4><<<(unsigned)tiles, 256, smem, s>>>(P);
+    else
+      fourier_sched_kernel<3><<<(unsigned)tiles, 256, smem, s>>>(P);
+  } else if (P.variant) {
     fourier_pass_kernel<4><<<(unsigned)tiles, 1 << (TB - 4), smem, s>>>(P);
-  else
+  } else {
     fourier_pass_kernel<3><<<(unsigned)tiles, 1 << (TB - 4), smem, s>>>(P);
+  }
   RGS_CUDA_TRY(cudaGetLastError());
   return RGS_OK;
 }
@@ -919,6 +1315,11 @@ void diag_tables(int m, int chunks, const std::vector<std::complex<double>>& f, 
 
 }  // namespace
 
+int fourier_set_register_schedule(int on) {
+  g_fourier_legacy = !on;
+  return RGS_OK;
+}
+
 std::string fourier_build(int n, const uint8_t* graph, const double* unitaries, int m, const int* A, const int* B,
                           bool deferred, FourierPlan& p, int& status) {
   status = RGS_ERR_ARG;
@@ -981,19 +1382,25 @@ std::string fourier_build(int n, const uint8_t* graph, const double* unitaries, 
   p.rot.assign((size_t)2 * m, 0.f);
   p.rot_ok = true;
   for (int j = 0; j < m && p.rot_ok; ++j) {
-    if (deferred && j == m - 1) {
-      p.rot[2 * j] = 1.f;
-      continue;
-    }
+    if (deferred && j == m - 1) continue;  // form 0 with k = 0: never applied
     std::complex<double> g2[2], h2[2];
     double c = 0.0, sn = 0.0;
     if (!euler_factors(&p.uA[(size_t)j * 8], g2, h2, c, sn)) p.rot_ok = false;
+    // R(c, s) = c [[1, -s/c], [s/c, 1]] (form 0) or s diag(-1, 1) [[-c/s, 1], [1, c/s]]
+    // (form 1); the scalar and diag(-1, 1) join the diagonal h applied after the products.
     fg[2 * j] = g2[0];
     fg[2 * j + 1] = g2[1];
-    fh[2 * j] = h2[0];
-    fh[2 * j + 1] = h2[1];
-    p.rot[2 * j] = (float)c;
-    p.rot[2 * j + 1] = (float)sn;
+    if (c >= sn) {
+      fh[2 * j] = h2[0] * c;
+      fh[2 * j + 1] = h2[1] * c;
+      p.rot[2 * j] = (float)(sn / c);
+      p.rot[2 * j + 1] = 0.f;
+    } else {
+      fh[2 * j] = -h2[0] * sn;
+      fh[2 * j + 1] = h2[1] * sn;
+      p.rot[2 * j] = (float)(c / sn);
+      p.rot[2 * j + 1] = 1.f;
+    }
   }
   if (p.rot_ok) {
     diag_tables(m, p.chunks, fg, p.dg);

@@ -39,7 +39,7 @@ struct FourierPlan {
   // diagonals (the deferred terminal bit has trivial factors).  rot_ok = false falls
   // back to general 2x2 products (a non-unitary input).
   bool rot_ok = false;
-  std::vector<float> rot;        // [m][2] (c, s)
+  std::vector<float> rot;        // [m][2] (k, form) of the scaled rotations (see fourier.cu)
   std::vector<float> dg, dh;     // [chunks][256][2] complex64 chunk products of g / h
   std::vector<float> rg, rh;     // [m][2] per-bit ratios g(1)/g(0), h(1)/h(0)
   TileTables tt_init{}, tt_phase{};         // pass tables of the init (pass 0) and of the q_A phase pass
@@ -86,13 +86,16 @@ struct FourierStages {
   float init_ms = 0, walsh_ms = 0, product_ms = 0;
 };
 
-// Full conditional state for outcome mask outB (bit j = outcome of B_j), in place in
-// `state` (complex64[2^m]); tile masses into the workspace.  If `stages` is given the
-// call synchronises and reports device time per stage.
 // Times one compute with each pass-kernel variant (after a warm-up) and keeps the faster
 // for this plan; ms[v] = milliseconds per compute (may be null).  Synchronises.
 int fourier_tune(FourierPlan& p, void* state, void* ws, size_t ws_bytes, cudaStream_t s, float* ms);
+// Passes of 12-bit tiles on the register-first kernel (on, default) or all passes on the
+// round-per-four-axes kernel (off).  Process-wide.
+int fourier_set_register_schedule(int on);
 
+// Full conditional state for outcome mask outB (bit j = outcome of B_j), in place in
+// `state` (complex64[2^m]); tile masses into the workspace.  If `stages` is given the
+// call synchronises and reports device time per stage.
 int fourier_compute(FourierPlan& p, uint64_t outB, void* state, void* ws, size_t ws_bytes, cudaStream_t s,
                     FourierStages* stages);
 // Reference pipeline (W/distributed_sampler.py:126-144, single device): product init over

@@ -240,3 +240,32 @@ def test_tensor_core_wht_rejects_small_states(pkg):
     d = torch.zeros(1 << 10, dtype=torch.complex64, device="cuda")
     with pytest.raises(NotImplementedError):
         pkg.fwht(d, precision="split_bf16x3")
+
+
+@pytest.mark.parametrize("m", [13, 16, 21, 22, 26, 29])
+@pytest.mark.parametrize("identical_b", [True, False])
+def test_register_schedule_matches_rounds(pkg, m, identical_b):
+    """The register-first pass kernel (default) and the one-round-per-four-axes kernel
+    give the same conditional state and tile masses.  m covers strided groups of 1 (m=13),
+    4, 9, 5+5, 7+7 and 9+8 target bits; identical B unitaries take the table init, Haar
+    ones the generic chunk init."""
+    g, u, A, B = _synthetic(pkg, m, 100 + m)
+    if identical_b:
+        u[B] = u[B[0]]
+    s = pkg.ConditionalSampler(g, u, A, B)
+    assert s.specialized == identical_b
+    ob = np.random.default_rng(m).integers(0, 2, m).tolist()
+    lib = pkg._lib.lib()
+    try:
+        pkg._lib.check(lib.rgs_fourier_set_register_schedule(0))
+        s.compute(ob)
+        ref = s.state.clone()
+        _, ref_norm, _, _ = s.masses()
+        pkg._lib.check(lib.rgs_fourier_set_register_schedule(1))
+        s.compute(ob)
+        _, norm, _, _ = s.masses()
+    finally:
+        pkg._lib.check(lib.rgs_fourier_set_register_schedule(1))
+    rel = float(torch.linalg.norm((s.state - ref).to(torch.complex128)) / torch.linalg.norm(ref.to(torch.complex128)))
+    assert rel < 1e-5, rel
+    assert abs(norm - ref_norm) < 1e-5 and abs(norm - 1) < 1e-4
