@@ -700,7 +700,7 @@ def run_chain(args, rank, world, local_rank, emit=True):
             "roofline": {"bound": "hbm", "achieved": bytes_per * BATCH * args.steps / t / 1e9,
                          "algorithmic_bytes_per_step": bytes_per * BATCH},
             "checks": {"max_abs_logp_minus_log_p": consistency, "linear_xeb": xeb},
-            "gpu_launches": args.steps * -(-BATCH // chain_tile) * (3 * N_QUBITS + 3),
+            "gpu_launches": args.steps * cs.launch_count(BATCH),
             "clocks": clocks.summary()}
     if emit and rank == 0:
         print(json.dumps(line), flush=True)

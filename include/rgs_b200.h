@@ -160,6 +160,11 @@ int rgs_scan_contract(rgs_plan* plan, const double* fvec, int64_t batch, int32_t
  * Workspace: rgs_chain_workspace_bytes().  check != 0 synchronises and reports a branch
  * pair of zero total mass as RGS_ERR_ZERO_NORM. */
 int rgs_chain_workspace_bytes(const rgs_plan* plan, int32_t batch_tile, int32_t precision, size_t* bytes);
+/* Kernel launches of one rgs_chain_sample (marginals = 0) or rgs_chain_marginals (1) call
+ * of `count` strings, with out_logp given (with_logp = 1) or NULL: the library's own
+ * schedule, counted without launching. */
+int rgs_chain_launch_count(const rgs_plan* plan, int64_t count, int32_t batch_tile, int32_t marginals,
+                           int32_t with_logp, int64_t* launches);
 /* count exact samples.  uniforms: device float64[count][n] in scan order, or NULL for
  * Philox4x32-10 uniforms keyed by seed (counter = item, position).
  * out_bits: device uint64[count][2]; out_value/out_logscale: the amplitude of each

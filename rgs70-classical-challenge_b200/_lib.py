@@ -86,6 +86,8 @@ SIGNATURES = {
     "rgs_scan_amplitudes_noalloc": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_int64, ctypes.c_int32,
                                                    c_void_p, c_void_p, c_void_p]),
     "rgs_chain_workspace_bytes": (ctypes.c_int, [c_void_p, ctypes.c_int32, ctypes.c_int32, c_size_t_p]),
+    "rgs_chain_launch_count": (ctypes.c_int, [c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
+                                              ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]),
     "rgs_chain_sample": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int64, ctypes.c_uint64, c_void_p, ctypes.c_int32,
                                         c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_size_t,
                                         ctypes.c_int32, ctypes.c_int32, c_void_p]),

@@ -70,6 +70,13 @@ class ChainSampler:
                 torch.empty(count, dtype=torch.float64, device=self.device),
                 torch.empty(count, dtype=torch.float64, device=self.device))
 
+    def launch_count(self, count, marginals=False, with_logp=True):
+        """Kernel launches of one sampling (or marginals) call of ``count`` strings."""
+        n = ctypes.c_int64()
+        _lib.check(_lib.lib().rgs_chain_launch_count(self.plan.handle, int(count), self.batch_tile,
+                                                     1 if marginals else 0, 1 if with_logp else 0, ctypes.byref(n)))
+        return int(n.value)
+
     def sample_device(self, count, seed=0, uniforms=None, check=True, stream=None, outs=None, cond=None):
         """Queue ``count`` samples; returns device tensors (bits, value, logscale, logp).
         ``cond``: optional float32 [count, n] device tensor for the conditionals met."""

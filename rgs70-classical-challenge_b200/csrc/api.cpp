@@ -271,6 +271,14 @@ int rgs_chain_workspace_bytes(const rgs_plan* plan, int32_t batch_tile, int32_t 
   return RGS_OK;
 }
 
+int rgs_chain_launch_count(const rgs_plan* plan, int64_t count, int32_t batch_tile, int32_t marginals,
+                           int32_t with_logp, int64_t* launches) {
+  if (!plan || !launches) return fail(RGS_ERR_ARG, "null argument");
+  if (count < 0 || batch_tile < 1) return fail(RGS_ERR_ARG, "count must be >= 0 and batch_tile >= 1");
+  *launches = (count + batch_tile - 1) / batch_tile * chain_launches_per_tile(plan->plan, marginals != 0, with_logp != 0);
+  return RGS_OK;
+}
+
 int rgs_chain_sample(rgs_plan* plan, const double* unitaries, int64_t count, uint64_t seed, const double* uniforms,
                      int32_t precision, uint64_t* out_bits, void* out_value, double* out_logscale, double* out_logp,
                      float* out_cond1, void* workspace, size_t workspace_bytes, int32_t batch_tile, int32_t check,

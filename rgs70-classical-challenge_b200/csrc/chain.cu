@@ -332,6 +332,27 @@ int chain_layout(const Plan& plan, int Bt, int precision, ChainLayout& L) {
   return RGS_OK;
 }
 
+// Kernel launches of chain_run per batch tile, following its schedule: bit clearing
+// (sampling) and log p zeroing (when asked), per position the Gram pass (unless analytic)
+// and the decision, per single position its scan step, per fused pair the pair Gram pass
+// (unless the second position is analytic) and the pair kernel, and the finalisation.
+long long chain_launches_per_tile(const Plan& plan, bool mode_given, bool with_logp) {
+  auto analytic = [&](int j) { return plan.dev[j].mode == MODE_PAIR && plan.dev[j].ncombos == 1; };
+  const bool fuse = !plan.pair_at.empty();
+  long long c = (mode_given ? 0 : 1) + (with_logp ? 1 : 0);
+  for (int j = 0; j < plan.n;) {
+    const int pa = fuse ? plan.pair_at[j] : -1;
+    if (pa >= 0 && j + 1 < plan.n) {
+      c += (analytic(j) ? 0 : 1) + 1 + (analytic(j + 1) ? 0 : 1) + 1 + 1;
+      j += 2;
+    } else {
+      c += (analytic(j) ? 0 : 1) + 1 + 1;
+      j += 1;
+    }
+  }
+  return c + 1;
+}
+
 int chain_run(Plan& plan, const double* U, long long count, int mode_given, u64 seed, const double* uniforms,
               int precision, unsigned long long* bits, void* out_value, double* out_logscale, double* out_logp,
               float* out_cond1, void* workspace, size_t ws_bytes, int Bt, cudaStream_t stream, bool check) {

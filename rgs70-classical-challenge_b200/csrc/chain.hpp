@@ -17,6 +17,8 @@ struct ChainLayout {
 
 int chain_max_tile(int precision);
 int chain_layout(const Plan& plan, int Bt, int precision, ChainLayout& L);
+// Kernel launches of chain_run per batch tile (sampling: mode_given = false).
+long long chain_launches_per_tile(const Plan& plan, bool mode_given, bool with_logp);
 
 // mode_given = 0: draw x (Philox(seed) uniforms, or `uniforms` [count][n] in scan
 // order); bits are written.  mode_given = 1: teacher forcing with the given bits.

@@ -32,6 +32,7 @@
 #include <cmath>
 #include <complex>
 #include <atomic>
+#include <type_traits>
 #include <mutex>
 
 #include "common.hpp"
@@ -110,6 +111,7 @@ struct PassParams {
   u64 ntiles;                     // tiles of this launch (0: every tile of the index space)
   int store_top;
   int sched;                      // 1: register-first schedule below (fourier_sched_kernel)
+  int top_axis;                   // tile axis at global bit m - 1, or -1 (sharded stores)
   PassSched s;
 };
 
@@ -560,13 +562,14 @@ __device__ __forceinline__ void reg_wht(float2 (&r)[16], const int (&ax)[4], uns
   }
 }
 
-__device__ __forceinline__ void reg_prod(float2 (&r)[16], const PassParams& P, const int (&ax)[4], unsigned um) {
+// srot[a] = the scaled rotation of tile axis a (shared, when P.rot).
+__device__ __forceinline__ void reg_prod(float2 (&r)[16], const PassParams& P, const float2* srot, const int (&ax)[4],
+                                         unsigned um) {
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     if (!((um >> ax[a]) & 1u)) continue;
-    const int gb = local_to_global_bit(P, ax[a]);
     if (P.rot) {
-      const float2 kf = __ldg(P.rot + gb);
+      const float2 kf = srot[ax[a]];
       const float2 k = make_float2(kf.x, kf.x), nk = make_float2(-kf.x, -kf.x);
       if (kf.y == 0.f) {
 #pragma unroll
@@ -578,7 +581,7 @@ __device__ __forceinline__ void reg_prod(float2 (&r)[16], const PassParams& P, c
           if (!(i & (1 << a))) apply_rot1(r[i], r[i | (1 << a)], k, nk);
       }
     } else {
-      const double2* u4 = P.u + 4 * gb;
+      const double2* u4 = P.u + 4 * local_to_global_bit(P, ax[a]);
       float2 uu[4];
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
@@ -592,17 +595,52 @@ __device__ __forceinline__ void reg_prod(float2 (&r)[16], const PassParams& P, c
   }
 }
 
-// q_A phase (pass tables) times the diagonal dg, on the registers; fof(i) = tile index.
-template <class F>
+// Register axes of the schedule's phase stage.
+__device__ __forceinline__ void phase_axes(const PassSched& S, int (&ax)[4]) {
+  const bool round = S.phase_at >= 1 && S.phase_at <= S.nr;
+  const bool l1 = S.phase_at == S.nr + 1 && S.fin_l1;
+  const int w0 = round ? S.rw0[S.phase_at - 1] : 0;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) ax[a] = round ? w0 + a : (a == 0 ? 0 : (l1 ? 5 : 8) + a);
+}
+
+// Tile-local part of a quadratic phase at tile index f (pass table bit, no tile constants).
+__device__ __forceinline__ int qt_bit(const TileTables& st, int f) { return (st.qtab[f >> 5] >> (f & 31)) & 1u; }
+
+// Signs (-1)^{q(f)} of a stage's 16 registers as a 16-bit mask, f = fb | X(i): the
+// thread's q(fb), the block's window part qw (bit i = qt(X) ^ parity(L & X), or 0 when the
+// caller folds it elsewhere) and the cross terms of q between fb and each axis.
+__device__ __forceinline__ unsigned sign_mask(const TileTables& st, int q0, unsigned lm, int fb,
+                                              const int (&ax)[4], unsigned qw) {
+  const unsigned pat[4] = {0xAAAAu, 0xCCCCu, 0xF0F0u, 0xFF00u};  // bit i set where i_a = 1
+  unsigned L = (tile_q(st, q0, lm, fb) ? 0xFFFFu : 0u) ^ qw;
+  const int qb = qt_bit(st, fb);
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int e = 1 << ax[a];
+    if (qt_bit(st, fb ^ e) ^ qb ^ qt_bit(st, e)) L ^= pat[a];
+  }
+  return L;
+}
+
+// q_A phase times the diagonal dg on the 16 registers of a stage, f = fb | X(i) with
+// X(i) = sum of i_a 2^{ax[a]} (fb: the thread's element 0, zero on the register axes).
+// dg is a product over bits and q is quadratic, so the factor of register i is
+//   dg(fb) * rt[i] * (-1)^{bit i of sign_mask(fb)}
+// with rt[i] = (-1)^{qt(X) ^ parity(L & X)} times the product of dg's per-bit ratios over
+// X (per block, shared): one shared broadcast load and two complex products per element
+// instead of a table walk and three.
 __device__ __forceinline__ void reg_phase(float2 (&r)[16], const PassParams& P, const float2 (*wt)[16],
-                                          const TileTables& st, int q0, unsigned lm, F fof) {
+                                          const TileTables& st, int q0, unsigned lm, const float2* rt, int fb) {
+  int ax[4];
+  phase_axes(P.s, ax);
+  const float2 F0 = P.dg ? window_factor(wt, fb) : make_float2(1.f, 0.f);
+  const unsigned L = sign_mask(st, q0, lm, fb, ax, 0u);
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
-    const int f = fof(i);
-    float2 x = r[i];
-    if (P.dg) x = cmulf(x, window_factor(wt, f));
-    if (tile_q(st, q0, lm, f)) x = make_float2(-x.x, -x.y);
-    r[i] = x;
+    float2 fac = cmulf(F0, rt[i]);
+    if ((L >> i) & 1u) fac = make_float2(-fac.x, -fac.y);
+    r[i] = cmulf(r[i], fac);
   }
 }
 
@@ -648,35 +686,43 @@ __device__ __forceinline__ int lay_f(int l1, int t, int i) {
   return l1 ? e + 2 * (t & 31) + 64 * k + 512 * (t >> 5) : e + 2 * t + 512 * k;
 }
 
-// Global offset of a tile bit, and the addresses of a layout: g(k) = g0 + sum of the
-// offsets of k's bits (tile_global is a sum over the bits of f).
-__device__ __forceinline__ u64 gbit(const PassParams& P, int b) {
-  return b < P.c ? (1ull << b) : (1ull << (P.q + b - P.c));
-}
-struct LayAddr {
-  u64 g0, d[3];
-};
-__device__ __forceinline__ LayAddr lay_addr(const PassParams& P, u64 tile, int l1) {
-  const int t = threadIdx.x;
-  LayAddr A;
-  A.g0 = tile_global(P, tile, lay_f(l1, t, 0));
-  const int kb = l1 ? 6 : 9;
-#pragma unroll
-  for (int j = 0; j < 3; ++j) A.d[j] = gbit(P, kb + j);
-  return A;
-}
-__device__ __forceinline__ u64 lay_g(const LayAddr& A, int k) {
-  return A.g0 + ((k & 1) ? A.d[0] : 0ull) + ((k & 2) ? A.d[1] : 0ull) + ((k & 4) ? A.d[2] : 0ull);
+// Element offset of tile index f from the tile's first element (tile_global is a sum
+// over the bits of f), with the shard mask applied.
+__device__ __forceinline__ u64 tile_off(const PassParams& P, int f) {
+  return ((u64)(f & ((1 << P.c) - 1)) | ((u64)(f >> P.c) << P.q)) & P.amask;
 }
 
-template <int MINB>
+// Offsets of a layout: element (k, e) of the thread sits at o0 + at(k) + e.  With m <= 32
+// (O = 32 bits) every offset fits and an access is one wide multiply-add from the tile
+// pointer; larger states use 64-bit offsets.
+template <typename O>
+struct LayOff {
+  O o0, d[3];
+  __device__ __forceinline__ O at(int k) const {
+    return o0 + ((k & 1) ? d[0] : (O)0) + ((k & 2) ? d[1] : (O)0) + ((k & 4) ? d[2] : (O)0);
+  }
+};
+template <typename O>
+__device__ __forceinline__ LayOff<O> lay_off(const PassParams& P, int l1) {
+  LayOff<O> A;
+  A.o0 = (O)tile_off(P, lay_f(l1, threadIdx.x, 0));
+  const int kb = l1 ? 6 : 9;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) A.d[j] = (O)tile_off(P, 1 << (kb + j));
+  return A;
+}
+
+template <int MINB, bool W64>
 __global__ void __launch_bounds__(256, MINB) fourier_sched_kernel(const __grid_constant__ PassParams P) {
+  using O = typename std::conditional<W64, u64, unsigned>::type;
   extern __shared__ float2 sm[];
   __shared__ float2 wt[3][16];  // window tables of the pass's diagonal (dg or dh)
   __shared__ TileTables s_tt;   // init or q_A pass tables
   __shared__ u64 s_b0;
   __shared__ int s_q0;
-  __shared__ unsigned s_lm;
+  __shared__ unsigned s_lm, s_qw;
+  __shared__ float2 s_rt[16];   // phase stage: per-block factors (see reg_phase)
+  __shared__ float2 s_rot[kTileBits];  // scaled rotation (k, form) per tile axis
   const PassSched& S = P.s;
   const int t = threadIdx.x;
   const u64 tile = blockIdx.x + P.tile0;
@@ -690,24 +736,63 @@ __global__ void __launch_bounds__(256, MINB) fourier_sched_kernel(const __grid_c
     window_tables(wt, P, P.dg, P.rg, base, kTileBits);
   else if (P.dh)
     window_tables(wt, P, P.dh, P.rh, base, kTileBits);
+  if (P.rot && t >= 64 && t < 64 + kTileBits) s_rot[t - 64] = __ldg(P.rot + local_to_global_bit(P, t - 64));
   __syncthreads();
   const int q0 = s_q0;
   const unsigned lm = s_lm;
+  const int ax0[4] = {0, 9, 10, 11};
+  if (init_tab || P.phase) {
+    // Per-block window parts of the quadratic phase: the init's (layout L0) as a sign
+    // mask, the q_A phase's folded into its factors rt.
+    if (t < 32) {
+      int pax[4] = {0, 9, 10, 11};
+      if (!init_tab) phase_axes(S, pax);
+      const int i = t & 15;
+      int X = 0;
+      float2 v = make_float2(1.f, 0.f);
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        if (!((i >> a) & 1)) continue;
+        X |= 1 << pax[a];
+        if (P.dg) v = cmulf(v, __ldg(P.rg + local_to_global_bit(P, pax[a])));
+      }
+      const int w = qt_bit(s_tt, X) ^ (__popc(lm & (unsigned)X) & 1);
+      const unsigned mask = __ballot_sync(0xffffffffu, t < 16 && w);
+      if (t == 0) s_qw = mask;
+      if (t < 16) s_rt[t] = w ? make_float2(-v.x, -v.y) : v;
+    }
+    __syncthreads();
+  }
   float2 r[16];
-  const LayAddr A0 = lay_addr(P, tile, 0);
   // Load stage (L0): init computed in registers, or the state loaded.
   if (init_tab) {
+    const unsigned sg = sign_mask(s_tt, q0, lm, 2 * t, ax0, s_qw);
     const u64 b0 = s_b0;
-    const u64 blo[2] = {b0 ^ s_tt.mlo[(2 * t) & 63], b0 ^ s_tt.mlo[(2 * t + 1) & 63]};
+    if (W64) {
+      const u64 blo[2] = {b0 ^ s_tt.mlo[(2 * t) & 63], b0 ^ s_tt.mlo[(2 * t + 1) & 63]};
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const u64 bhi = s_tt.mhi[((2 * t + 512 * k) >> 6) & 63];
+      for (int k = 0; k < 8; ++k) {
+        const u64 bhi = s_tt.mhi[((2 * t + 512 * k) >> 6) & 63];
 #pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int f = lay_f(0, t, 2 * k + e);
-        const u64 b = blo[e] ^ bhi;
-        const float2 w = __ldg(P.wspecf + __popcll(b) * (P.m + 1) + __popcll(b & P.outmask));
-        r[2 * k + e] = tile_q(s_tt, q0, lm, f) ? make_float2(-w.x, -w.y) : w;
+        for (int e = 0; e < 2; ++e) {
+          const u64 b = blo[e] ^ bhi;
+          const float2 w = __ldg(P.wspecf + __popcll(b) * (P.m + 1) + __popcll(b & P.outmask));
+          r[2 * k + e] = ((sg >> (2 * k + e)) & 1u) ? make_float2(-w.x, -w.y) : w;
+        }
+      }
+    } else {
+      // m <= 32: b and the outcome mask fit 32 bits.
+      const unsigned out = (unsigned)P.outmask;
+      const unsigned blo[2] = {(unsigned)(b0 ^ s_tt.mlo[(2 * t) & 63]), (unsigned)(b0 ^ s_tt.mlo[(2 * t + 1) & 63])};
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const unsigned bhi = (unsigned)s_tt.mhi[((2 * t + 512 * k) >> 6) & 63];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const unsigned b = blo[e] ^ bhi;
+          const float2 w = __ldg(P.wspecf + __popc(b) * (P.m + 1) + __popc(b & out));
+          r[2 * k + e] = ((sg >> (2 * k + e)) & 1u) ? make_float2(-w.x, -w.y) : w;
+        }
       }
     }
   } else if (P.init) {
@@ -716,22 +801,23 @@ __global__ void __launch_bounds__(256, MINB) fourier_sched_kernel(const __grid_c
     tile_lut(P.lut_z, P.chunks, base, varying, tl);
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      const u64 g = lay_g(A0, k);
+      const u64 g = tile_global(P, tile, lay_f(0, t, 2 * k));
       r[2 * k] = init_value(P, tl, g);
       r[2 * k + 1] = init_value(P, tl, g + 1);
     }
   } else {
+    const float2* vt = P.v + (base & P.amask);
+    const LayOff<O> A = lay_off<O>(P, 0);
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      const float4 x = *reinterpret_cast<const float4*>(P.v + (lay_g(A0, k) & P.amask));
+      const float4 x = *reinterpret_cast<const float4*>(vt + A.at(k));
       r[2 * k] = make_float2(x.x, x.y);
       r[2 * k + 1] = make_float2(x.z, x.w);
     }
   }
-  const int ax0[4] = {0, 9, 10, 11};
   reg_wht(r, ax0, S.ld_w);
-  if (P.phase && S.phase_at == 0) reg_phase(r, P, wt, s_tt, q0, lm, [&](int i) { return lay_f(0, t, i); });
-  reg_prod(r, P, ax0, S.ld_u);
+  if (P.phase && S.phase_at == 0) reg_phase(r, P, wt, s_tt, q0, lm, s_rt, lay_f(0, t, 0));
+  reg_prod(r, P, s_rot, ax0, S.ld_u);
   const int fl = S.fin_l1;
   if (S.nr > 0 || fl) {
     float2* b0p = sm + pad(2 * t);
@@ -743,11 +829,8 @@ __global__ void __launch_bounds__(256, MINB) fourier_sched_kernel(const __grid_c
       round_io_at<false>(sm, r, w0);
       const int ax[4] = {w0, w0 + 1, w0 + 2, w0 + 3};
       reg_wht(r, ax, S.rw[j]);
-      if (P.phase && S.phase_at == j + 1) {
-        const int f0 = round_f0(t, w0);
-        reg_phase(r, P, wt, s_tt, q0, lm, [&](int i) { return f0 | (i << w0); });
-      }
-      reg_prod(r, P, ax, S.ru[j]);
+      if (P.phase && S.phase_at == j + 1) reg_phase(r, P, wt, s_tt, q0, lm, s_rt, round_f0(t, w0));
+      reg_prod(r, P, s_rot, ax, S.ru[j]);
       round_io_at<true>(sm, r, w0);
     }
     __syncthreads();
@@ -757,8 +840,8 @@ __global__ void __launch_bounds__(256, MINB) fourier_sched_kernel(const __grid_c
   }
   const int axf[4] = {0, fl ? 6 : 9, fl ? 7 : 10, fl ? 8 : 11};
   reg_wht(r, axf, S.fw);
-  if (P.phase && S.phase_at == S.nr + 1) reg_phase(r, P, wt, s_tt, q0, lm, [&](int i) { return lay_f(fl, t, i); });
-  reg_prod(r, P, axf, S.fu);
+  if (P.phase && S.phase_at == S.nr + 1) reg_phase(r, P, wt, s_tt, q0, lm, s_rt, lay_f(fl, t, 0));
+  reg_prod(r, P, s_rot, axf, S.fu);
   // Diagonal after the products (final layout L0 only), masses, store.
   if (P.dh) {
     const WindowSplit ws = window_split(wt, 256);
@@ -769,14 +852,20 @@ __global__ void __launch_bounds__(256, MINB) fourier_sched_kernel(const __grid_c
       r[2 * k + 1] = cmulf(r[2 * k + 1], window_factor(wt, ws, f, 1));
     }
   }
-  const LayAddr Af = lay_addr(P, tile, fl);  // recomputed: A0 is not kept live across the rounds
+  float2* vt = P.v + (base & P.amask);
+  const LayOff<O> Af = lay_off<O>(P, fl);
+  // Sharded pass 0 stores only the elements whose top bit (m - 1) equals store_top.
+  const int base_top = (int)((base >> (P.m - 1)) & 1ull);
   double mass = 0.0;  // per element pair: a float sum of four squares, then float64
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    const u64 g = lay_g(Af, k);
     const float2 a = r[2 * k], b = r[2 * k + 1];
-    if (P.store && (P.store_top < 0 || (int)((g >> (P.m - 1)) & 1ull) == P.store_top))
-      *reinterpret_cast<float4*>(P.v + (g & P.amask)) = make_float4(a.x, a.y, b.x, b.y);
+    bool st = P.store != 0;
+    if (P.store_top >= 0) {
+      const int top = P.top_axis >= 0 ? base_top ^ ((lay_f(fl, t, 2 * k) >> P.top_axis) & 1) : base_top;
+      st = st && top == P.store_top;
+    }
+    if (st) *reinterpret_cast<float4*>(vt + Af.at(k)) = make_float4(a.x, a.y, b.x, b.y);
     if (P.masses) {
       const float2 q = f2fma(b, b, make_float2(a.x * a.x, a.y * a.y));
       mass += (double)(q.x + q.y);
@@ -1007,7 +1096,10 @@ int set_smem_attr() {
   if (device >= 0 && device < 64 && done[device]) return RGS_OK;
   const int bytes = ((1 << kTileBits) + (1 << (kTileBits - 4))) * (int)sizeof(float2);
   RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_pass_kernel<MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_sched_kernel<MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  RGS_CUDA_TRY(
+      cudaFuncSetAttribute(fourier_sched_kernel<MINB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  RGS_CUDA_TRY(
+      cudaFuncSetAttribute(fourier_sched_kernel<MINB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   if (device >= 0 && device < 64) done[device] = true;
   return RGS_OK;
 }
@@ -1083,11 +1175,20 @@ int launch_pass(const PassParams& Pin, cudaStream_t s) {
   // diagonal and not both the init and the phase.
   P.sched = TB == kTileBits && !(P.init && P.phase) && !(P.phase && !P.tt_phase) && !(P.dg && P.dh) &&
             !g_fourier_legacy && plan_sched(P, P.s);
+  P.top_axis = -1;
+  for (int a = 0; a < TB; ++a)
+    if ((a < P.c ? a : P.q + (a - P.c)) == P.m - 1) P.top_axis = a;
   if (P.sched) {
-    if (P.variant)
-      fourier_sched_kernel<4><<<(unsigned)tiles, 256, smem, s>>>(P);
+    // 32-bit element offsets inside a tile while the state has at most 2^32 elements.
+    const bool w64 = P.m > 32;
+    if (P.variant && w64)
+      fourier_sched_kernel<4, true><<<(unsigned)tiles, 256, smem, s>>>(P);
+    else if (P.variant)
+      fourier_sched_kernel<4, false><<<(unsigned)tiles, 256, smem, s>>>(P);
+    else if (w64)
+      fourier_sched_kernel<3, true><<<(unsigned)tiles, 256, smem, s>>>(P);
     else
-      fourier_sched_kernel<3><<<(unsigned)tiles, 256, smem, s>>>(P);
+      fourier_sched_kernel<3, false><<<(unsigned)tiles, 256, smem, s>>>(P);
   } else if (P.variant) {
     fourier_pass_kernel<4><<<(unsigned)tiles, 1 << (TB - 4), smem, s>>>(P);
   } else {

@@ -102,3 +102,22 @@ def test_chain_errors(pkg):
         cs.sample(4)
     with pytest.raises(ValueError):
         pkg.ChainSampler(inst.g, inst.u, inst.order).sample(4, uniforms=np.zeros((3, 10)))
+
+
+@pytest.mark.parametrize("kind,n,seed", [("reg3", 12, 1), ("deg3", 16, 4)])
+def test_launch_count_matches_profiler(pkg, kind, n, seed):
+    """rgs_chain_launch_count (the benchmark's gpu_launches) equals the kernels that the
+    CUDA profiler sees for one sampling call: 3 batch tiles, with log p."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    inst = _instance(pkg, kind, n, seed)
+    cs = pkg.ChainSampler(inst.g, inst.u, inst.order, precision="c64f32", batch_tile=32)
+    count = 3 * cs.batch_tile
+    outs = cs._outs(count)
+    cs.sample_device(count, seed=1, check=False, outs=outs)
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        cs.sample_device(count, seed=2, check=False, outs=outs)
+        torch.cuda.synchronize()
+    ours = sum(e.count for e in prof.key_averages() if "_kernel" in e.key)
+    assert ours == cs.launch_count(count) == 3 * cs.launch_count(cs.batch_tile)
