@@ -599,6 +599,7 @@ def run_fourier(args, rank, world, local_rank):
     g, u, A, B = fourier_instance(pkg, m)
     L = pkg._lib.lib()
     pkg._lib.check(L.rgs_fourier_set_register_schedule(1 if args.pass_kernel == "registers" else 0))
+    pkg._lib.check(L.rgs_fourier_set_tma(1 if args.tma else 0))
     s = pkg.ConditionalSampler(g, u, A, B, [local_rank])
     variant, tune_ms = s.tune()
     stream = torch.cuda.current_stream(device)
@@ -637,6 +638,7 @@ def run_fourier(args, rank, world, local_rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded dense graph)",
             "config": {"workload": f"conditional sampler, dense graph n={2 * m}, full-rank balanced cut m={m}",
                        "passes": s.passes, "specialized": s.specialized, "pass_kernel": args.pass_kernel,
+                       "tile_loads": "tma" if args.tma and args.pass_kernel == "registers" else "threads",
                        "tuned_variant": {"chosen": variant, "ms_per_compute": tune_ms,
                                          "variants": "3 or 4 resident blocks per SM"}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -1266,6 +1268,8 @@ def main():
     ap.add_argument("--order", choices=["searched", "random"], default="searched",
                     help="scan order of the learned workload's n=56 instance")
     ap.add_argument("--m", type=int, default=30, help="conditional qubits of the fourier workload")
+    ap.add_argument("--tma", action="store_true",
+                    help="fourier workload: stage tiles with TMA loads in persistent blocks (default: thread loads)")
     ap.add_argument("--pass-kernel", choices=["registers", "rounds"], default="registers",
                     help="fourier workload: register-first pass kernel (default) or one shared-memory "
                          "round per four axes")

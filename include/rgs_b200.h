@@ -261,6 +261,13 @@ int rgs_fourier_tune(rgs_fourier* plan, void* state, void* workspace, size_t wor
  * operations per axis, in a different order across axes (FP32 results agree to rounding).
  * Exists for tests and measurements.  Process-wide. */
 int rgs_fourier_set_register_schedule(int32_t on);
+/* Loading passes of the register-first kernel: tiles staged by tensor-map (TMA) loads in
+ * persistent blocks, the next tile in flight while the current one is transformed (1), or
+ * loaded by the threads with 16-byte accesses (0, default: faster on B200, where the
+ * staging buffer leaves room for three resident blocks per SM instead of four).  Both
+ * read the same values into the same registers (bit-identical results).  A staged pass
+ * whose bounded wait gives up is reported by rgs_tensor_core_status.  Process-wide. */
+int rgs_fourier_set_tma(int32_t on);
 /* The reference base pipeline (distributed_sampler.py:126-144): product init over b,
  * WHT, index map with q_A phase into `scratch`, products; result in `scratch`. */
 int rgs_fourier_compute_permute(rgs_fourier* plan, uint64_t outB, void* state, void* scratch, void* workspace,
@@ -322,8 +329,9 @@ int rgs_block_mass(const void* state, int32_t nbits, int32_t tile_bits, double* 
 int rgs_gemm_bf16(int32_t M, int32_t N, int32_t K, const void* A, int32_t lda, int32_t transA, const void* B,
                   int32_t ldb, int32_t transB, float alpha, const float* bias, int32_t relu, const uint8_t* mask,
                   const void* gate, float* C, void* Cb, int32_t ldc, void* stream);
-/* *timed_out = 1 if a bounded wait of a tensor-core kernel (GEMM, tensor-core Hadamard
- * passes) gave up since the last call (its results are then invalid); clears the flag.
+/* *timed_out = 1 if a bounded wait of a tensor-core or TMA-staged kernel (GEMM,
+ * tensor-core Hadamard passes, TMA-staged Fourier passes) gave up since the last call (its
+ * results are then invalid); clears the flag.
  * Synchronous. */
 int rgs_tensor_core_status(int32_t* timed_out);
 /* TMA loads of the GEMM's K-major operands with 16-byte aligned rows: on (1, default) or

@@ -110,6 +110,7 @@ SIGNATURES = {
     "rgs_tensor_core_status": (ctypes.c_int, [c_int32_p]),
     "rgs_gemm_set_tma": (ctypes.c_int, [ctypes.c_int32]),
     "rgs_fourier_set_register_schedule": (ctypes.c_int, [ctypes.c_int32]),
+    "rgs_fourier_set_tma": (ctypes.c_int, [ctypes.c_int32]),
     "rgs_mlp_fwd": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32] + [c_void_p] * 11),
     "rgs_mlp_bwd": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32] + [c_void_p] * 20
                     + [ctypes.c_int32, c_void_p]),

@@ -101,6 +101,8 @@ int rgs_fourier_tune(rgs_fourier* f, void* state, void* workspace, size_t worksp
 
 int rgs_fourier_set_register_schedule(int32_t on) { return fourier_set_register_schedule(on); }
 
+int rgs_fourier_set_tma(int32_t on) { return fourier_set_tma(on); }
+
 int rgs_fourier_compute(rgs_fourier* f, uint64_t outB, void* state, void* workspace, size_t workspace_bytes,
                         void* stream, float* stage_ms) {
   if (!f) return fail(RGS_ERR_ARG, "plan is NULL");

@@ -10,11 +10,16 @@
 // distributed_sampler.py:50-54, 145-157; deferred_global_sampler.py:65-78).
 //
 // Pass structure.  The state is 2^m complex64 values in HBM.  A pass streams it once
-// in tiles of 2^12 elements staged in shared memory (four 256-thread blocks per SM):
-// either a contiguous tile (the 12 low bits) or a strided tile (at least 3 contiguous
-// low bits = 64-byte runs, times up to 9 "target" bits at position q).  Inside a tile each thread holds 16 elements in
-// registers along 4 tile axes and applies every 2x2 operation on those axes; four-axis
-// rounds are separated by a swizzled shared-memory exchange.  The whole transform is
+// in tiles of 2^12 elements (three or four 256-thread blocks per SM): either a contiguous
+// tile (the 12 low bits) or a strided tile (at least 3 contiguous low bits = 64-byte runs,
+// times up to 9 "target" bits at position q).  Inside a tile each thread holds 16
+// elements in registers along 4 tile axes and applies every 2x2 operation on those axes.
+// fourier_sched_kernel (12-bit tiles) transforms the axes that sit in registers right
+// after the load and before the store there, and the rest in at most three padded
+// shared-memory rounds chosen per pass by the host (plan_sched); its loading passes stage
+// each next tile with a tensor-map (TMA) load while the current one is transformed.
+// fourier_pass_kernel (tiles of fewer bits, the generic phase path) runs one round per
+// four axes.  The whole transform is
 //   pass 0          : init (computed, not loaded) + WHT on bits [0, 12)
 //   strided passes  : WHT on the next groups of <= 9 bits (balanced)
 //   middle pass     : WHT on the last group, q_A phase, products on that group
@@ -32,14 +37,20 @@
 #include <cmath>
 #include <complex>
 #include <atomic>
+#include <cstring>
 #include <type_traits>
 #include <mutex>
 
 #include "common.hpp"
 #include "f32x2.cuh"
 #include "fourier.cuh"
+#include "tcgen05.cuh"
+#include "tma_map.hpp"
 
 namespace rgs {
+
+// Set when a bounded wait of a TMA-staged pass gave up (read by tensor_core_status).
+__device__ int g_fourier_timeout = 0;
 
 typedef unsigned long long u64;
 
@@ -112,8 +123,14 @@ struct PassParams {
   int store_top;
   int sched;                      // 1: register-first schedule below (fourier_sched_kernel)
   int top_axis;                   // tile axis at global bit m - 1, or -1 (sharded stores)
+  int tma_mid_dim, tma_high_dim;  // tensor-map dimensions of the mid and high index bits, or -1
   PassSched s;
 };
+
+// Shared memory of a pass: the padded work buffer (kWorkElems float2), and for the
+// TMA-staged kernel a dense staging buffer behind it (1024-byte aligned).
+constexpr int kWorkElems = (1 << kTileBits) + (1 << (kTileBits - 4));
+constexpr size_t kTmaSmemBytes = kWorkElems * sizeof(float2) + 1024 + (sizeof(float2) << kTileBits);
 
 // Padded shared-memory layout: one spare slot per 16 elements, so the 16 threads of a
 // half-warp hit distinct 8-byte bank pairs in every access pattern used here, and a
@@ -548,37 +565,48 @@ __global__ void __launch_bounds__(256, MINB) fourier_pass_kernel(const __grid_co
 // after it.  Against one shared-memory round per four axes this saves up to two
 // exchanges per element and pass (four in the middle pass).
 
-__device__ __forceinline__ void reg_wht(float2 (&r)[16], const int (&ax)[4], unsigned wm) {
+// The registers hold each complex value as one 64-bit pair (v2, f32x2.cuh), the operand
+// form of the packed FP32 instructions.
+__device__ __forceinline__ void reg_wht(v2 (&r)[16], const int (&ax)[4], unsigned wm) {
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     if (!((wm >> ax[a]) & 1u)) continue;
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
       if (i & (1 << a)) continue;
-      const float2 x = r[i], y = r[i | (1 << a)];
-      r[i] = f2add(x, y);
-      r[i | (1 << a)] = f2sub(x, y);
+      const v2 x = r[i], y = r[i | (1 << a)];
+      r[i] = v2add(x, y);
+      r[i | (1 << a)] = v2sub(x, y);
     }
   }
 }
 
 // srot[a] = the scaled rotation of tile axis a (shared, when P.rot).
-__device__ __forceinline__ void reg_prod(float2 (&r)[16], const PassParams& P, const float2* srot, const int (&ax)[4],
+__device__ __forceinline__ void reg_prod(v2 (&r)[16], const PassParams& P, const float2* srot, const int (&ax)[4],
                                          unsigned um) {
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     if (!((um >> ax[a]) & 1u)) continue;
     if (P.rot) {
+      // Scaled rotation, one packed FMA per output (see apply_rot0 / apply_rot1).
       const float2 kf = srot[ax[a]];
-      const float2 k = make_float2(kf.x, kf.x), nk = make_float2(-kf.x, -kf.x);
+      const v2 k = v2pack(make_float2(kf.x, kf.x)), nk = v2pack(make_float2(-kf.x, -kf.x));
       if (kf.y == 0.f) {
 #pragma unroll
-        for (int i = 0; i < 16; ++i)
-          if (!(i & (1 << a))) apply_rot0(r[i], r[i | (1 << a)], k, nk);
+        for (int i = 0; i < 16; ++i) {
+          if (i & (1 << a)) continue;
+          const v2 x = r[i], y = r[i | (1 << a)];
+          r[i] = v2fma(nk, y, x);
+          r[i | (1 << a)] = v2fma(k, x, y);
+        }
       } else {
 #pragma unroll
-        for (int i = 0; i < 16; ++i)
-          if (!(i & (1 << a))) apply_rot1(r[i], r[i | (1 << a)], k, nk);
+        for (int i = 0; i < 16; ++i) {
+          if (i & (1 << a)) continue;
+          const v2 x = r[i], y = r[i | (1 << a)];
+          r[i] = v2fma(nk, x, y);
+          r[i | (1 << a)] = v2fma(k, y, x);
+        }
       }
     } else {
       const double2* u4 = P.u + 4 * local_to_global_bit(P, ax[a]);
@@ -589,8 +617,13 @@ __device__ __forceinline__ void reg_prod(float2 (&r)[16], const PassParams& P, c
         uu[e] = make_float2((float)d.x, (float)d.y);
       }
 #pragma unroll
-      for (int i = 0; i < 16; ++i)
-        if (!(i & (1 << a))) apply_u(r[i], r[i | (1 << a)], uu);
+      for (int i = 0; i < 16; ++i) {
+        if (i & (1 << a)) continue;
+        float2 x = v2unpack(r[i]), y = v2unpack(r[i | (1 << a)]);
+        apply_u(x, y, uu);
+        r[i] = v2pack(x);
+        r[i | (1 << a)] = v2pack(y);
+      }
     }
   }
 }
@@ -630,7 +663,7 @@ __device__ __forceinline__ unsigned sign_mask(const TileTables& st, int q0, unsi
 // with rt[i] = (-1)^{qt(X) ^ parity(L & X)} times the product of dg's per-bit ratios over
 // X (per block, shared): one shared broadcast load and two complex products per element
 // instead of a table walk and three.
-__device__ __forceinline__ void reg_phase(float2 (&r)[16], const PassParams& P, const float2 (*wt)[16],
+__device__ __forceinline__ void reg_phase(v2 (&r)[16], const PassParams& P, const float2 (*wt)[16],
                                           const TileTables& st, int q0, unsigned lm, const float2* rt, int fb) {
   int ax[4];
   phase_axes(P.s, ax);
@@ -640,7 +673,7 @@ __device__ __forceinline__ void reg_phase(float2 (&r)[16], const PassParams& P, 
   for (int i = 0; i < 16; ++i) {
     float2 fac = cmulf(F0, rt[i]);
     if ((L >> i) & 1u) fac = make_float2(-fac.x, -fac.y);
-    r[i] = cmulf(r[i], fac);
+    r[i] = v2pack(cmulf(v2unpack(r[i]), fac));
   }
 }
 
@@ -650,8 +683,8 @@ __device__ __forceinline__ int round_f0(int t) {
 }
 
 template <int W0, bool STORE>
-__device__ __forceinline__ void round_io(float2* sm, float2 (&r)[16]) {
-  float2* b = sm + pad(round_f0<W0>(threadIdx.x));
+__device__ __forceinline__ void round_io(float2* sm, v2 (&r)[16]) {
+  v2* b = reinterpret_cast<v2*>(sm) + pad(round_f0<W0>(threadIdx.x));
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
     if (STORE)
@@ -662,7 +695,7 @@ __device__ __forceinline__ void round_io(float2* sm, float2 (&r)[16]) {
 }
 
 template <bool STORE>
-__device__ __forceinline__ void round_io_at(float2* sm, float2 (&r)[16], int w0) {
+__device__ __forceinline__ void round_io_at(float2* sm, v2 (&r)[16], int w0) {
   switch (w0) {
     case 0: round_io<0, STORE>(sm, r); break;
     case 1: round_io<1, STORE>(sm, r); break;
@@ -712,10 +745,33 @@ __device__ __forceinline__ LayOff<O> lay_off(const PassParams& P, int l1) {
   return A;
 }
 
-template <int MINB, bool W64>
-__global__ void __launch_bounds__(256, MINB) fourier_sched_kernel(const __grid_constant__ PassParams P) {
+// Issues the tensor-map load of tile `tile` into the staging buffer (one thread).  The
+// map's dimensions (innermost first) follow the index bits: the tile's low bits, the mid
+// bits [c, q), the target bits, the high bits [q + K, ...) -- boxes are full on the tile's
+// dimensions and 1 on the others, so the box lands in tile index order.
+__device__ __forceinline__ void tma_tile(const PassParams& P, const CUtensorMap& map, u64 tile, float2* stage,
+                                         uint64_t* bar) {
+  const u64 bm = tile_global(P, tile, 0) & P.amask;
+  int c[5] = {0, 0, 0, 0, 0};
+  if (P.tma_mid_dim >= 0) c[P.tma_mid_dim] = (int)((bm >> P.c) & ((1ull << (P.q - P.c)) - 1ull));
+  if (P.tma_high_dim >= 0) c[P.tma_high_dim] = (int)(bm >> (P.q + P.K));
+  tc::mbar_expect_tx(bar, (uint32_t)(sizeof(float2) << kTileBits));
+  tc::tma_load_5d(stage, &map, c[0], c[1], c[2], c[3], c[4], bar);
+}
+
+// TMA = true: a persistent loop over the launch's tiles (tile blockIdx.x + i gridDim.x) in
+// which one thread prefetches the next tile with a tensor-map load into a dense staging
+// buffer while the block transforms the current one; the load stage then reads the tile
+// from shared memory (16-byte accesses, layout L0) instead of from HBM.
+template <int MINB, bool W64, bool TMA>
+__global__ void __launch_bounds__(256, MINB)
+    fourier_sched_kernel(const __grid_constant__ PassParams P, const __grid_constant__ CUtensorMap tmap) {
   using O = typename std::conditional<W64, u64, unsigned>::type;
   extern __shared__ float2 sm[];
+  // TMA staging buffer (dense tile) after the padded work buffer, 1024-byte aligned.
+  const uint32_t sa = tc::smem_u32(sm + kWorkElems);
+  float2* stage = sm + kWorkElems + ((((sa + 1023u) & ~1023u) - sa) / sizeof(float2));
+  __shared__ __align__(8) uint64_t s_full;
   __shared__ float2 wt[3][16];  // window tables of the pass's diagonal (dg or dh)
   __shared__ TileTables s_tt;   // init or q_A pass tables
   __shared__ u64 s_b0;
@@ -725,9 +781,21 @@ __global__ void __launch_bounds__(256, MINB) fourier_sched_kernel(const __grid_c
   __shared__ float2 s_rot[kTileBits];  // scaled rotation (k, form) per tile axis
   const PassSched& S = P.s;
   const int t = threadIdx.x;
-  const u64 tile = blockIdx.x + P.tile0;
-  const u64 base = tile_global(P, tile, 0);
+  const u64 ntl = P.ntiles ? P.ntiles : (1ull << (P.m - kTileBits));
   const bool init_tab = P.init == INIT_COV_SPECIAL && P.tt_init;
+  uint32_t phase = 0;
+  if (TMA) {
+    if (t == 0) {
+      tc::mbar_init(&s_full, 1);
+      tc::fence_barrier_init();
+    }
+    __syncthreads();
+    if (t == 0 && blockIdx.x < ntl) tma_tile(P, tmap, blockIdx.x + P.tile0, stage, &s_full);
+  }
+  for (u64 it = blockIdx.x; it < ntl; it += TMA ? gridDim.x : ntl) {
+  const u64 tile = it + P.tile0;
+  const u64 base = tile_global(P, tile, 0);
+  if (TMA) __syncthreads();  // the previous tile's readers of the shared tables and buffers are done
   if (init_tab)
     tile_tables_setup(P, P.tt_init, P.lut_z, P.qsym_z, base, kTileBits, true, s_tt, s_b0, s_q0, s_lm);
   else if (P.phase)
@@ -763,7 +831,7 @@ __global__ void __launch_bounds__(256, MINB) fourier_sched_kernel(const __grid_c
     }
     __syncthreads();
   }
-  float2 r[16];
+  v2 r[16];
   // Load stage (L0): init computed in registers, or the state loaded.
   if (init_tab) {
     const unsigned sg = sign_mask(s_tt, q0, lm, 2 * t, ax0, s_qw);
@@ -777,7 +845,7 @@ __global__ void __launch_bounds__(256, MINB) fourier_sched_kernel(const __grid_c
         for (int e = 0; e < 2; ++e) {
           const u64 b = blo[e] ^ bhi;
           const float2 w = __ldg(P.wspecf + __popcll(b) * (P.m + 1) + __popcll(b & P.outmask));
-          r[2 * k + e] = ((sg >> (2 * k + e)) & 1u) ? make_float2(-w.x, -w.y) : w;
+          r[2 * k + e] = v2pack(((sg >> (2 * k + e)) & 1u) ? make_float2(-w.x, -w.y) : w);
         }
       }
     } else {
@@ -791,7 +859,7 @@ __global__ void __launch_bounds__(256, MINB) fourier_sched_kernel(const __grid_c
         for (int e = 0; e < 2; ++e) {
           const unsigned b = blo[e] ^ bhi;
           const float2 w = __ldg(P.wspecf + __popc(b) * (P.m + 1) + __popc(b & out));
-          r[2 * k + e] = ((sg >> (2 * k + e)) & 1u) ? make_float2(-w.x, -w.y) : w;
+          r[2 * k + e] = v2pack(((sg >> (2 * k + e)) & 1u) ? make_float2(-w.x, -w.y) : w);
         }
       }
     }
@@ -802,17 +870,38 @@ __global__ void __launch_bounds__(256, MINB) fourier_sched_kernel(const __grid_c
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const u64 g = tile_global(P, tile, lay_f(0, t, 2 * k));
-      r[2 * k] = init_value(P, tl, g);
-      r[2 * k + 1] = init_value(P, tl, g + 1);
+      r[2 * k] = v2pack(init_value(P, tl, g));
+      r[2 * k + 1] = v2pack(init_value(P, tl, g + 1));
     }
+  } else if (TMA) {
+    // The tile is in the staging buffer (dense, tile index order): wait for it, read it,
+    // then refill the buffer with the next tile while this one is transformed.  A wait
+    // that gives up sets the error flag and ends the block (uniformly).
+    const bool ok = tc::mbar_wait(&s_full, phase);
+    phase ^= 1;
+    if (__syncthreads_or(!ok)) {
+      if (t == 0) {
+        atomicExch(&g_fourier_timeout, 1);
+        tc::mbar_wait(&s_full, phase ^ 1);  // bounded: the copy in flight, if any
+      }
+      return;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(stage + 2 * t + 512 * k);
+      r[2 * k] = x.x;
+      r[2 * k + 1] = x.y;
+    }
+    __syncthreads();
+    if (t == 0 && it + gridDim.x < ntl) tma_tile(P, tmap, it + gridDim.x + P.tile0, stage, &s_full);
   } else {
     const float2* vt = P.v + (base & P.amask);
     const LayOff<O> A = lay_off<O>(P, 0);
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      const float4 x = *reinterpret_cast<const float4*>(vt + A.at(k));
-      r[2 * k] = make_float2(x.x, x.y);
-      r[2 * k + 1] = make_float2(x.z, x.w);
+      const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(vt + A.at(k));
+      r[2 * k] = x.x;
+      r[2 * k + 1] = x.y;
     }
   }
   reg_wht(r, ax0, S.ld_w);
@@ -820,7 +909,7 @@ __global__ void __launch_bounds__(256, MINB) fourier_sched_kernel(const __grid_c
   reg_prod(r, P, s_rot, ax0, S.ld_u);
   const int fl = S.fin_l1;
   if (S.nr > 0 || fl) {
-    float2* b0p = sm + pad(2 * t);
+    v2* b0p = reinterpret_cast<v2*>(sm) + pad(2 * t);
 #pragma unroll
     for (int i = 0; i < 16; ++i) b0p[(i & 1) + 544 * (i >> 1)] = r[i];
     for (int j = 0; j < S.nr; ++j) {
@@ -834,7 +923,7 @@ __global__ void __launch_bounds__(256, MINB) fourier_sched_kernel(const __grid_c
       round_io_at<true>(sm, r, w0);
     }
     __syncthreads();
-    float2* bf = sm + pad(lay_f(fl, t, 0));
+    const v2* bf = reinterpret_cast<const v2*>(sm) + pad(lay_f(fl, t, 0));
 #pragma unroll
     for (int i = 0; i < 16; ++i) r[i] = bf[(i & 1) + (fl ? 68 : 544) * (i >> 1)];
   }
@@ -848,8 +937,8 @@ __global__ void __launch_bounds__(256, MINB) fourier_sched_kernel(const __grid_c
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const int f = lay_f(0, t, 2 * k);
-      r[2 * k] = cmulf(r[2 * k], window_factor(wt, ws, f, 0));
-      r[2 * k + 1] = cmulf(r[2 * k + 1], window_factor(wt, ws, f, 1));
+      r[2 * k] = v2pack(cmulf(v2unpack(r[2 * k]), window_factor(wt, ws, f, 0)));
+      r[2 * k + 1] = v2pack(cmulf(v2unpack(r[2 * k + 1]), window_factor(wt, ws, f, 1)));
     }
   }
   float2* vt = P.v + (base & P.amask);
@@ -859,13 +948,13 @@ __global__ void __launch_bounds__(256, MINB) fourier_sched_kernel(const __grid_c
   double mass = 0.0;  // per element pair: a float sum of four squares, then float64
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    const float2 a = r[2 * k], b = r[2 * k + 1];
+    const float2 a = v2unpack(r[2 * k]), b = v2unpack(r[2 * k + 1]);
     bool st = P.store != 0;
     if (P.store_top >= 0) {
       const int top = P.top_axis >= 0 ? base_top ^ ((lay_f(fl, t, 2 * k) >> P.top_axis) & 1) : base_top;
       st = st && top == P.store_top;
     }
-    if (st) *reinterpret_cast<float4*>(vt + Af.at(k)) = make_float4(a.x, a.y, b.x, b.y);
+    if (st) *reinterpret_cast<ulonglong2*>(vt + Af.at(k)) = make_ulonglong2(r[2 * k], r[2 * k + 1]);
     if (P.masses) {
       const float2 q = f2fma(b, b, make_float2(a.x * a.x, a.y * a.y));
       mass += (double)(q.x + q.y);
@@ -883,6 +972,8 @@ __global__ void __launch_bounds__(256, MINB) fourier_sched_kernel(const __grid_c
       P.masses[tile - P.tile0] = sum;
     }
   }
+  if (!TMA) break;  // one tile per block
+  }  // tiles
 }
 
 // Per-sample weight tables: generic chunk products over b (with 2^{-m/2} in chunk 0)
@@ -1086,6 +1177,53 @@ __global__ void __launch_bounds__(1024) shard_mass_kernel(const double* __restri
 // ------------------------------------------------------------------------------------- host
 std::mutex g_fourier_mutex;
 std::atomic<bool> g_fourier_legacy{false};  // true: every pass on fourier_pass_kernel
+std::atomic<bool> g_fourier_tma{false};     // TMA-staged loads of the register-first passes (opt-in)
+
+// Tensor map of a loading pass's tiles over the state buffer (8-byte elements): the index
+// bits in runs -- the tile's low bits [0, c), the mid bits [c, q), the target bits
+// [q, q + K), the high bits -- runs of tile bits split at 8 bits (box dimensions <= 256),
+// boxes full on tile runs and 1 elsewhere.  False when the geometry does not fit five
+// dimensions or the TMA limits (then the pass loads with plain 16-byte accesses).
+bool tma_pass_map(PassParams& P, CUtensorMap* map) {
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc || ((uintptr_t)P.v & 15) != 0) return false;
+  const int mm = P.amask == ~0ull ? P.m : P.m - 1;  // index bits of the buffer
+  if (P.q + P.K > mm) return false;
+  struct Run {
+    int lo, bits;
+    bool tile;
+  };
+  std::vector<Run> runs;
+  auto tile_run = [&](int lo, int bits) {
+    for (int b = 0; b < bits; b += 8) runs.push_back({lo + b, std::min(8, bits - b), true});
+  };
+  tile_run(0, P.c);
+  P.tma_mid_dim = P.tma_high_dim = -1;
+  if (P.q > P.c) {
+    P.tma_mid_dim = (int)runs.size();
+    runs.push_back({P.c, P.q - P.c, false});
+  }
+  tile_run(P.q, P.K);
+  if (mm > P.q + P.K) {
+    P.tma_high_dim = (int)runs.size();
+    runs.push_back({P.q + P.K, mm - P.q - P.K, false});
+  }
+  if (runs.size() > 5) return false;
+  cuuint64_t dims[5], strides[4];
+  cuuint32_t box[5], estr[5] = {1, 1, 1, 1, 1};
+  for (int d = 0; d < 5; ++d) {
+    const bool real = d < (int)runs.size();
+    dims[d] = real ? (1ull << runs[d].bits) : 1ull;
+    box[d] = real && runs[d].tile ? (1u << runs[d].bits) : 1u;
+    if (d > 0) {
+      strides[d - 1] = real ? (8ull << runs[d].lo) : 16ull;
+      if (strides[d - 1] >= (1ull << 40) || dims[d] > (1ull << 32)) return false;
+    }
+  }
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 5, (void*)P.v, dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 template <int MINB>
 int set_smem_attr() {
@@ -1096,10 +1234,16 @@ int set_smem_attr() {
   if (device >= 0 && device < 64 && done[device]) return RGS_OK;
   const int bytes = ((1 << kTileBits) + (1 << (kTileBits - 4))) * (int)sizeof(float2);
   RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_pass_kernel<MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  RGS_CUDA_TRY(
-      cudaFuncSetAttribute(fourier_sched_kernel<MINB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  RGS_CUDA_TRY(
-      cudaFuncSetAttribute(fourier_sched_kernel<MINB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_sched_kernel<MINB, false, false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_sched_kernel<MINB, true, false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  if (MINB == 3) {
+    RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_sched_kernel<3, false, true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmemBytes));
+    RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_sched_kernel<3, true, true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmemBytes));
+  }
   if (device >= 0 && device < 64) done[device] = true;
   return RGS_OK;
 }
@@ -1181,14 +1325,30 @@ int launch_pass(const PassParams& Pin, cudaStream_t s) {
   if (P.sched) {
     // 32-bit element offsets inside a tile while the state has at most 2^32 elements.
     const bool w64 = P.m > 32;
-    if (P.variant && w64)
-      fourier_sched_kernel<4, true><<<(unsigned)tiles, 256, smem, s>>>(P);
-    else if (P.variant)
-      fourier_sched_kernel<4, false><<<(unsigned)tiles, 256, smem, s>>>(P);
-    else if (w64)
-      fourier_sched_kernel<3, true><<<(unsigned)tiles, 256, smem, s>>>(P);
-    else
-      fourier_sched_kernel<3, false><<<(unsigned)tiles, 256, smem, s>>>(P);
+    CUtensorMap map;
+    std::memset(&map, 0, sizeof(map));
+    if (!P.init && g_fourier_tma && tma_pass_map(P, &map)) {
+      // TMA-staged persistent blocks: three per SM (work + staging buffers).
+      if (P.variant) {
+        const int rc3 = set_smem_attr<3>();
+        if (rc3) return rc3;
+      }
+      int dev = 0;
+      RGS_CUDA_TRY(cudaGetDevice(&dev));
+      const unsigned grid = (unsigned)std::min<u64>(tiles, (u64)3 * sm_count(dev));
+      if (w64)
+        fourier_sched_kernel<3, true, true><<<grid, 256, kTmaSmemBytes, s>>>(P, map);
+      else
+        fourier_sched_kernel<3, false, true><<<grid, 256, kTmaSmemBytes, s>>>(P, map);
+    } else if (P.variant && w64) {
+      fourier_sched_kernel<4, true, false><<<(unsigned)tiles, 256, smem, s>>>(P, map);
+    } else if (P.variant) {
+      fourier_sched_kernel<4, false, false><<<(unsigned)tiles, 256, smem, s>>>(P, map);
+    } else if (w64) {
+      fourier_sched_kernel<3, true, false><<<(unsigned)tiles, 256, smem, s>>>(P, map);
+    } else {
+      fourier_sched_kernel<3, false, false><<<(unsigned)tiles, 256, smem, s>>>(P, map);
+    }
   } else if (P.variant) {
     fourier_pass_kernel<4><<<(unsigned)tiles, 1 << (TB - 4), smem, s>>>(P);
   } else {
@@ -1418,6 +1578,19 @@ void diag_tables(int m, int chunks, const std::vector<std::complex<double>>& f, 
 
 int fourier_set_register_schedule(int on) {
   g_fourier_legacy = !on;
+  return RGS_OK;
+}
+
+int fourier_set_tma(int on) {
+  g_fourier_tma = on != 0;
+  return RGS_OK;
+}
+
+int fourier_tma_timeout(int* timed_out) {
+  int h = 0, zero = 0;
+  RGS_CUDA_TRY(cudaMemcpyFromSymbol(&h, g_fourier_timeout, sizeof(int)));
+  RGS_CUDA_TRY(cudaMemcpyToSymbol(g_fourier_timeout, &zero, sizeof(int)));
+  *timed_out = h;
   return RGS_OK;
 }
 

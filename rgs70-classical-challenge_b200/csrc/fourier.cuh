@@ -92,6 +92,12 @@ int fourier_tune(FourierPlan& p, void* state, void* ws, size_t ws_bytes, cudaStr
 // Passes of 12-bit tiles on the register-first kernel (on, default) or all passes on the
 // round-per-four-axes kernel (off).  Process-wide.
 int fourier_set_register_schedule(int on);
+// Loading passes of the register-first kernel stage their tiles with tensor-map (TMA)
+// loads in persistent blocks (on) or load them with 16-byte accesses (off, default: the
+// faster on B200, where the staging buffer costs a resident block per SM).
+int fourier_set_tma(int on);
+// Whether a bounded wait of a TMA-staged pass gave up since the last call; clears it.
+int fourier_tma_timeout(int* timed_out);
 
 // Full conditional state for outcome mask outB (bit j = outcome of B_j), in place in
 // `state` (complex64[2^m]); tile masses into the workspace.  If `stages` is given the

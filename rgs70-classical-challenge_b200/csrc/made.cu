@@ -16,6 +16,7 @@
 #include "common.hpp"
 #include "made.hpp"
 #include "tcgen05.cuh"
+#include "tma_map.hpp"
 
 namespace rgs {
 
@@ -23,6 +24,7 @@ namespace rgs {
 __device__ int g_tc_timeout = 0;
 
 int wht_tensor_core_timeout(int* timed_out);
+int fourier_tma_timeout(int* timed_out);
 
 namespace {
 
@@ -302,25 +304,6 @@ __global__ void logq_kernel(const float* __restrict__ z, const __nv_bfloat16* __
 }  // namespace
 
 namespace {
-// cuTensorMapEncodeTiled through the runtime's driver entry point (the library does not
-// link the driver, so it loads on machines without one).
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-EncodeTiledFn encode_tiled() {
-  static EncodeTiledFn fn = []() -> EncodeTiledFn {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess) {
-      cudaGetLastError();
-      return nullptr;
-    }
-    return (EncodeTiledFn)p;
-  }();
-  return fn;
-}
-
 // Tensor map of a K-major bf16 operand [rows][ld] (K innermost): boxes of 64 x 128 with
 // 128-byte swizzle, zero fill outside the operand.  False when TMA cannot load it (row
 // pitch not a multiple of 16 bytes, unaligned base, or no encoder).
@@ -370,10 +353,11 @@ int tensor_core_status(int* timed_out) {
   int h = 0, zero = 0;
   RGS_CUDA_TRY(cudaMemcpyFromSymbol(&h, g_tc_timeout, sizeof(int)));
   RGS_CUDA_TRY(cudaMemcpyToSymbol(g_tc_timeout, &zero, sizeof(int)));
-  int w = 0;
+  int w = 0, f = 0;
   int rc = wht_tensor_core_timeout(&w);
   if (rc) return rc;
-  *timed_out = h | w;
+  if ((rc = fourier_tma_timeout(&f))) return rc;
+  *timed_out = h | w | f;
   return RGS_OK;
 }
 

@@ -269,3 +269,27 @@ def test_register_schedule_matches_rounds(pkg, m, identical_b):
     rel = float(torch.linalg.norm((s.state - ref).to(torch.complex128)) / torch.linalg.norm(ref.to(torch.complex128)))
     assert rel < 1e-5, rel
     assert abs(norm - ref_norm) < 1e-5 and abs(norm - 1) < 1e-4
+
+
+@pytest.mark.parametrize("m", [13, 21, 26, 29])
+def test_tma_staging_is_bit_identical(pkg, m):
+    """TMA-staged tile loads and thread loads (default) read the same values into the
+    same registers: the conditional state is bit-identical, and no bounded wait gave up."""
+    import ctypes
+    g, u, A, B = _synthetic(pkg, m, 200 + m)
+    u[B] = u[B[0]]
+    s = pkg.ConditionalSampler(g, u, A, B)
+    ob = np.random.default_rng(m).integers(0, 2, m).tolist()
+    lib = pkg._lib.lib()
+    try:
+        pkg._lib.check(lib.rgs_fourier_set_tma(0))
+        s.compute(ob)
+        ref = s.state.clone()
+        pkg._lib.check(lib.rgs_fourier_set_tma(1))
+        s.compute(ob)
+    finally:
+        pkg._lib.check(lib.rgs_fourier_set_tma(0))
+    assert torch.equal(s.state, ref)
+    flag = ctypes.c_int32()
+    pkg._lib.check(lib.rgs_tensor_core_status(ctypes.byref(flag)))
+    assert flag.value == 0
