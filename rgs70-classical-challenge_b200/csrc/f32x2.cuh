@@ -44,39 +44,3 @@ __device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) {
 }
 #endif
 
-// The same operations on a (re, im) pair held as one 64-bit register (v2): a pass keeps
-// its registers in this form, so the packed instructions need no pairing moves.
-typedef unsigned long long v2;
-
-__device__ __forceinline__ v2 v2pack(float2 a) {
-  v2 d;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(a.x), "f"(a.y));
-  return d;
-}
-__device__ __forceinline__ float2 v2unpack(v2 a) {
-  float2 d;
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(d.x), "=f"(d.y) : "l"(a));
-  return d;
-}
-#ifndef RGS_NO_F32X2
-__device__ __forceinline__ v2 v2add(v2 a, v2 b) {
-  v2 d;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ v2 v2sub(v2 a, v2 b) {
-  v2 d;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-// a * b + c per lane.
-__device__ __forceinline__ v2 v2fma(v2 a, v2 b, v2 c) {
-  v2 d;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-  return d;
-}
-#else
-__device__ __forceinline__ v2 v2add(v2 a, v2 b) { return v2pack(f2add(v2unpack(a), v2unpack(b))); }
-__device__ __forceinline__ v2 v2sub(v2 a, v2 b) { return v2pack(f2sub(v2unpack(a), v2unpack(b))); }
-__device__ __forceinline__ v2 v2fma(v2 a, v2 b, v2 c) { return v2pack(f2fma(v2unpack(a), v2unpack(b), v2unpack(c))); }
-#endif

@@ -565,48 +565,37 @@ __global__ void __launch_bounds__(256, MINB) fourier_pass_kernel(const __grid_co
 // after it.  Against one shared-memory round per four axes this saves up to two
 // exchanges per element and pass (four in the middle pass).
 
-// The registers hold each complex value as one 64-bit pair (v2, f32x2.cuh), the operand
-// form of the packed FP32 instructions.
-__device__ __forceinline__ void reg_wht(v2 (&r)[16], const int (&ax)[4], unsigned wm) {
+__device__ __forceinline__ void reg_wht(float2 (&r)[16], const int (&ax)[4], unsigned wm) {
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     if (!((wm >> ax[a]) & 1u)) continue;
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
       if (i & (1 << a)) continue;
-      const v2 x = r[i], y = r[i | (1 << a)];
-      r[i] = v2add(x, y);
-      r[i | (1 << a)] = v2sub(x, y);
+      const float2 x = r[i], y = r[i | (1 << a)];
+      r[i] = f2add(x, y);
+      r[i | (1 << a)] = f2sub(x, y);
     }
   }
 }
 
 // srot[a] = the scaled rotation of tile axis a (shared, when P.rot).
-__device__ __forceinline__ void reg_prod(v2 (&r)[16], const PassParams& P, const float2* srot, const int (&ax)[4],
+__device__ __forceinline__ void reg_prod(float2 (&r)[16], const PassParams& P, const float2* srot, const int (&ax)[4],
                                          unsigned um) {
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     if (!((um >> ax[a]) & 1u)) continue;
     if (P.rot) {
-      // Scaled rotation, one packed FMA per output (see apply_rot0 / apply_rot1).
       const float2 kf = srot[ax[a]];
-      const v2 k = v2pack(make_float2(kf.x, kf.x)), nk = v2pack(make_float2(-kf.x, -kf.x));
+      const float2 k = make_float2(kf.x, kf.x), nk = make_float2(-kf.x, -kf.x);
       if (kf.y == 0.f) {
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          if (i & (1 << a)) continue;
-          const v2 x = r[i], y = r[i | (1 << a)];
-          r[i] = v2fma(nk, y, x);
-          r[i | (1 << a)] = v2fma(k, x, y);
-        }
+        for (int i = 0; i < 16; ++i)
+          if (!(i & (1 << a))) apply_rot0(r[i], r[i | (1 << a)], k, nk);
       } else {
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          if (i & (1 << a)) continue;
-          const v2 x = r[i], y = r[i | (1 << a)];
-          r[i] = v2fma(nk, x, y);
-          r[i | (1 << a)] = v2fma(k, y, x);
-        }
+        for (int i = 0; i < 16; ++i)
+          if (!(i & (1 << a))) apply_rot1(r[i], r[i | (1 << a)], k, nk);
       }
     } else {
       const double2* u4 = P.u + 4 * local_to_global_bit(P, ax[a]);
@@ -617,13 +606,8 @@ __device__ __forceinline__ void reg_prod(v2 (&r)[16], const PassParams& P, const
         uu[e] = make_float2((float)d.x, (float)d.y);
       }
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        if (i & (1 << a)) continue;
-        float2 x = v2unpack(r[i]), y = v2unpack(r[i | (1 << a)]);
-        apply_u(x, y, uu);
-        r[i] = v2pack(x);
-        r[i | (1 << a)] = v2pack(y);
-      }
+      for (int i = 0; i < 16; ++i)
+        if (!(i & (1 << a))) apply_u(r[i], r[i | (1 << a)], uu);
     }
   }
 }
@@ -663,7 +647,7 @@ __device__ __forceinline__ unsigned sign_mask(const TileTables& st, int q0, unsi
 // with rt[i] = (-1)^{qt(X) ^ parity(L & X)} times the product of dg's per-bit ratios over
 // X (per block, shared): one shared broadcast load and two complex products per element
 // instead of a table walk and three.
-__device__ __forceinline__ void reg_phase(v2 (&r)[16], const PassParams& P, const float2 (*wt)[16],
+__device__ __forceinline__ void reg_phase(float2 (&r)[16], const PassParams& P, const float2 (*wt)[16],
                                           const TileTables& st, int q0, unsigned lm, const float2* rt, int fb) {
   int ax[4];
   phase_axes(P.s, ax);
@@ -673,7 +657,7 @@ __device__ __forceinline__ void reg_phase(v2 (&r)[16], const PassParams& P, cons
   for (int i = 0; i < 16; ++i) {
     float2 fac = cmulf(F0, rt[i]);
     if ((L >> i) & 1u) fac = make_float2(-fac.x, -fac.y);
-    r[i] = v2pack(cmulf(v2unpack(r[i]), fac));
+    r[i] = cmulf(r[i], fac);
   }
 }
 
@@ -683,8 +667,8 @@ __device__ __forceinline__ int round_f0(int t) {
 }
 
 template <int W0, bool STORE>
-__device__ __forceinline__ void round_io(float2* sm, v2 (&r)[16]) {
-  v2* b = reinterpret_cast<v2*>(sm) + pad(round_f0<W0>(threadIdx.x));
+__device__ __forceinline__ void round_io(float2* sm, float2 (&r)[16]) {
+  float2* b = sm + pad(round_f0<W0>(threadIdx.x));
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
     if (STORE)
@@ -695,7 +679,7 @@ __device__ __forceinline__ void round_io(float2* sm, v2 (&r)[16]) {
 }
 
 template <bool STORE>
-__device__ __forceinline__ void round_io_at(float2* sm, v2 (&r)[16], int w0) {
+__device__ __forceinline__ void round_io_at(float2* sm, float2 (&r)[16], int w0) {
   switch (w0) {
     case 0: round_io<0, STORE>(sm, r); break;
     case 1: round_io<1, STORE>(sm, r); break;
@@ -831,7 +815,7 @@ __global__ void __launch_bounds__(256, MINB)
     }
     __syncthreads();
   }
-  v2 r[16];
+  float2 r[16];
   // Load stage (L0): init computed in registers, or the state loaded.
   if (init_tab) {
     const unsigned sg = sign_mask(s_tt, q0, lm, 2 * t, ax0, s_qw);
@@ -845,7 +829,7 @@ __global__ void __launch_bounds__(256, MINB)
         for (int e = 0; e < 2; ++e) {
           const u64 b = blo[e] ^ bhi;
           const float2 w = __ldg(P.wspecf + __popcll(b) * (P.m + 1) + __popcll(b & P.outmask));
-          r[2 * k + e] = v2pack(((sg >> (2 * k + e)) & 1u) ? make_float2(-w.x, -w.y) : w);
+          r[2 * k + e] = ((sg >> (2 * k + e)) & 1u) ? make_float2(-w.x, -w.y) : w;
         }
       }
     } else {
@@ -859,7 +843,7 @@ __global__ void __launch_bounds__(256, MINB)
         for (int e = 0; e < 2; ++e) {
           const unsigned b = blo[e] ^ bhi;
           const float2 w = __ldg(P.wspecf + __popc(b) * (P.m + 1) + __popc(b & out));
-          r[2 * k + e] = v2pack(((sg >> (2 * k + e)) & 1u) ? make_float2(-w.x, -w.y) : w);
+          r[2 * k + e] = ((sg >> (2 * k + e)) & 1u) ? make_float2(-w.x, -w.y) : w;
         }
       }
     }
@@ -870,8 +854,8 @@ __global__ void __launch_bounds__(256, MINB)
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const u64 g = tile_global(P, tile, lay_f(0, t, 2 * k));
-      r[2 * k] = v2pack(init_value(P, tl, g));
-      r[2 * k + 1] = v2pack(init_value(P, tl, g + 1));
+      r[2 * k] = init_value(P, tl, g);
+      r[2 * k + 1] = init_value(P, tl, g + 1);
     }
   } else if (TMA) {
     // The tile is in the staging buffer (dense, tile index order): wait for it, read it,
@@ -888,9 +872,9 @@ __global__ void __launch_bounds__(256, MINB)
     }
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(stage + 2 * t + 512 * k);
-      r[2 * k] = x.x;
-      r[2 * k + 1] = x.y;
+      const float4 x = *reinterpret_cast<const float4*>(stage + 2 * t + 512 * k);
+      r[2 * k] = make_float2(x.x, x.y);
+      r[2 * k + 1] = make_float2(x.z, x.w);
     }
     __syncthreads();
     if (t == 0 && it + gridDim.x < ntl) tma_tile(P, tmap, it + gridDim.x + P.tile0, stage, &s_full);
@@ -899,9 +883,9 @@ __global__ void __launch_bounds__(256, MINB)
     const LayOff<O> A = lay_off<O>(P, 0);
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(vt + A.at(k));
-      r[2 * k] = x.x;
-      r[2 * k + 1] = x.y;
+      const float4 x = *reinterpret_cast<const float4*>(vt + A.at(k));
+      r[2 * k] = make_float2(x.x, x.y);
+      r[2 * k + 1] = make_float2(x.z, x.w);
     }
   }
   reg_wht(r, ax0, S.ld_w);
@@ -909,7 +893,7 @@ __global__ void __launch_bounds__(256, MINB)
   reg_prod(r, P, s_rot, ax0, S.ld_u);
   const int fl = S.fin_l1;
   if (S.nr > 0 || fl) {
-    v2* b0p = reinterpret_cast<v2*>(sm) + pad(2 * t);
+    float2* b0p = sm + pad(2 * t);
 #pragma unroll
     for (int i = 0; i < 16; ++i) b0p[(i & 1) + 544 * (i >> 1)] = r[i];
     for (int j = 0; j < S.nr; ++j) {
@@ -923,7 +907,7 @@ __global__ void __launch_bounds__(256, MINB)
       round_io_at<true>(sm, r, w0);
     }
     __syncthreads();
-    const v2* bf = reinterpret_cast<const v2*>(sm) + pad(lay_f(fl, t, 0));
+    float2* bf = sm + pad(lay_f(fl, t, 0));
 #pragma unroll
     for (int i = 0; i < 16; ++i) r[i] = bf[(i & 1) + (fl ? 68 : 544) * (i >> 1)];
   }
@@ -937,8 +921,8 @@ __global__ void __launch_bounds__(256, MINB)
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const int f = lay_f(0, t, 2 * k);
-      r[2 * k] = v2pack(cmulf(v2unpack(r[2 * k]), window_factor(wt, ws, f, 0)));
-      r[2 * k + 1] = v2pack(cmulf(v2unpack(r[2 * k + 1]), window_factor(wt, ws, f, 1)));
+      r[2 * k] = cmulf(r[2 * k], window_factor(wt, ws, f, 0));
+      r[2 * k + 1] = cmulf(r[2 * k + 1], window_factor(wt, ws, f, 1));
     }
   }
   float2* vt = P.v + (base & P.amask);
@@ -948,13 +932,13 @@ __global__ void __launch_bounds__(256, MINB)
   double mass = 0.0;  // per element pair: a float sum of four squares, then float64
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    const float2 a = v2unpack(r[2 * k]), b = v2unpack(r[2 * k + 1]);
+    const float2 a = r[2 * k], b = r[2 * k + 1];
     bool st = P.store != 0;
     if (P.store_top >= 0) {
       const int top = P.top_axis >= 0 ? base_top ^ ((lay_f(fl, t, 2 * k) >> P.top_axis) & 1) : base_top;
       st = st && top == P.store_top;
     }
-    if (st) *reinterpret_cast<ulonglong2*>(vt + Af.at(k)) = make_ulonglong2(r[2 * k], r[2 * k + 1]);
+    if (st) *reinterpret_cast<float4*>(vt + Af.at(k)) = make_float4(a.x, a.y, b.x, b.y);
     if (P.masses) {
       const float2 q = f2fma(b, b, make_float2(a.x * a.x, a.y * a.y));
       mass += (double)(q.x + q.y);
