@@ -347,8 +347,18 @@ def run_ours(args, rank, world, local_rank):
     v64, l64 = eng64.out_tensors(BATCH) if use64 else (None, None)
     v128, l128 = eng128.out_tensors(BATCH) if use128 else (None, None)
     stream = torch.cuda.current_stream(device)
+    side = torch.cuda.Stream(device)
 
     def queue_step(s):
+        # The complex64 bulk and the complex128 recheck are independent sweeps over the
+        # same strings: the recheck runs on a second stream (a parallel branch of the step's
+        # graph), so each sweep's kernels fill the other's launch tails.
+        if use64 and use128 and not args.serial_sweeps:
+            side.wait_stream(s)
+            eng128.run_bits(d_bits, v128, l128, stream=side)
+            eng64.run_bits(d_bits, v64, l64, stream=s)
+            s.wait_stream(side)
+            return
         if use64:
             eng64.run_bits(d_bits, v64, l64, stream=s)
         if use128:
@@ -541,7 +551,10 @@ def run_ours(args, rank, world, local_rank):
                        "bulk": ("complex64 tables, float32 arithmetic" if args.bulk == "c64f32"
                                 else "complex64 tables, float64 arithmetic (the reference recipe)"),
                        "recheck": "complex128 tables, float64 arithmetic, every result",
-                       "launch": "each precision's sweep replayed from a CUDA graph",
+                       "launch": ("the two sweeps replayed from one CUDA graph, one after the other"
+                                  if args.serial_sweeps else
+                                  "the two sweeps replayed from one CUDA graph, the recheck on a parallel "
+                                  "branch (second stream)"),
                        "l2": "inputs larger than L2 (tables of 2^20 rows x batch tile, >= 2 x 1 GiB)",
                        "parallelism": f"replicas x{world}"},
             "split": {f"{args.bulk}_amplitudes_per_s": world * BATCH * args.steps / t64 if t64 else None,
@@ -1277,6 +1290,8 @@ def main():
     ap.add_argument("--bulk", choices=["c64f32", "c64"], default="c64f32",
                     help="complex64 bulk arithmetic: float32 (default) or float64")
     ap.add_argument("--no-alt", action="store_true", help="skip timing the other complex64 recipe")
+    ap.add_argument("--serial-sweeps", action="store_true",
+                    help="run the complex64 bulk and the complex128 recheck one after the other")
     ap.add_argument("--tile128", type=int, default=None, help="complex128 batch tile (default: autotuned)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
