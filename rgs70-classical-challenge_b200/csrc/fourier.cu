@@ -579,35 +579,23 @@ __device__ __forceinline__ void reg_wht(float2 (&r)[16], const int (&ax)[4], uns
   }
 }
 
-// srot[a] = the scaled rotation of tile axis a (shared, when P.rot).
+// srot[a] = the scaled rotation of tile axis a (shared); the register-first kernel runs
+// products only as scaled rotations (general 2x2 products take fourier_pass_kernel).
 __device__ __forceinline__ void reg_prod(float2 (&r)[16], const PassParams& P, const float2* srot, const int (&ax)[4],
                                          unsigned um) {
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     if (!((um >> ax[a]) & 1u)) continue;
-    if (P.rot) {
-      const float2 kf = srot[ax[a]];
-      const float2 k = make_float2(kf.x, kf.x), nk = make_float2(-kf.x, -kf.x);
-      if (kf.y == 0.f) {
-#pragma unroll
-        for (int i = 0; i < 16; ++i)
-          if (!(i & (1 << a))) apply_rot0(r[i], r[i | (1 << a)], k, nk);
-      } else {
-#pragma unroll
-        for (int i = 0; i < 16; ++i)
-          if (!(i & (1 << a))) apply_rot1(r[i], r[i | (1 << a)], k, nk);
-      }
-    } else {
-      const double2* u4 = P.u + 4 * local_to_global_bit(P, ax[a]);
-      float2 uu[4];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const double2 d = __ldg(u4 + e);
-        uu[e] = make_float2((float)d.x, (float)d.y);
-      }
+    const float2 kf = srot[ax[a]];
+    const float2 k = make_float2(kf.x, kf.x), nk = make_float2(-kf.x, -kf.x);
+    if (kf.y == 0.f) {
 #pragma unroll
       for (int i = 0; i < 16; ++i)
-        if (!(i & (1 << a))) apply_u(r[i], r[i | (1 << a)], uu);
+        if (!(i & (1 << a))) apply_rot0(r[i], r[i | (1 << a)], k, nk);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 16; ++i)
+        if (!(i & (1 << a))) apply_rot1(r[i], r[i | (1 << a)], k, nk);
     }
   }
 }
@@ -792,7 +780,6 @@ __global__ void __launch_bounds__(256, MINB)
   __syncthreads();
   const int q0 = s_q0;
   const unsigned lm = s_lm;
-  const int ax0[4] = {0, 9, 10, 11};
   if (init_tab || P.phase) {
     // Per-block window parts of the quadratic phase: the init's (layout L0) as a sign
     // mask, the q_A phase's folded into its factors rt.
@@ -818,6 +805,7 @@ __global__ void __launch_bounds__(256, MINB)
   float2 r[16];
   // Load stage (L0): init computed in registers, or the state loaded.
   if (init_tab) {
+    const int ax0[4] = {0, 9, 10, 11};
     const unsigned sg = sign_mask(s_tt, q0, lm, 2 * t, ax0, s_qw);
     const u64 b0 = s_b0;
     if (W64) {
@@ -888,33 +876,46 @@ __global__ void __launch_bounds__(256, MINB)
       r[2 * k + 1] = make_float2(x.z, x.w);
     }
   }
-  reg_wht(r, ax0, S.ld_w);
-  if (P.phase && S.phase_at == 0) reg_phase(r, P, wt, s_tt, q0, lm, s_rt, lay_f(0, t, 0));
-  reg_prod(r, P, s_rot, ax0, S.ld_u);
+  // Stages 0 (load, L0), 1..nr (shared-memory rounds) and nr + 1 (final, L0 or L1) share
+  // one copy of the register operations (a rolled loop): the kernel's code stays small
+  // enough for the instruction cache.
   const int fl = S.fin_l1;
-  if (S.nr > 0 || fl) {
-    float2* b0p = sm + pad(2 * t);
-#pragma unroll
-    for (int i = 0; i < 16; ++i) b0p[(i & 1) + 544 * (i >> 1)] = r[i];
-    for (int j = 0; j < S.nr; ++j) {
+  const bool exchange = S.nr > 0 || fl;
+#pragma unroll 1
+  for (int st = 0; st <= S.nr + 1; ++st) {
+    int ax[4];
+    unsigned wm, um;
+    int fb;
+    if (st == 0) {
+      ax[0] = 0, ax[1] = 9, ax[2] = 10, ax[3] = 11;
+      wm = S.ld_w, um = S.ld_u, fb = 2 * t;
+    } else if (st <= S.nr) {
+      const int w0 = S.rw0[st - 1];
+      ax[0] = w0, ax[1] = w0 + 1, ax[2] = w0 + 2, ax[3] = w0 + 3;
+      wm = S.rw[st - 1], um = S.ru[st - 1], fb = round_f0(t, w0);
       __syncthreads();
-      const int w0 = S.rw0[j];
       round_io_at<false>(sm, r, w0);
-      const int ax[4] = {w0, w0 + 1, w0 + 2, w0 + 3};
-      reg_wht(r, ax, S.rw[j]);
-      if (P.phase && S.phase_at == j + 1) reg_phase(r, P, wt, s_tt, q0, lm, s_rt, round_f0(t, w0));
-      reg_prod(r, P, s_rot, ax, S.ru[j]);
-      round_io_at<true>(sm, r, w0);
-    }
-    __syncthreads();
-    float2* bf = sm + pad(lay_f(fl, t, 0));
+    } else {
+      ax[0] = 0, ax[1] = fl ? 6 : 9, ax[2] = fl ? 7 : 10, ax[3] = fl ? 8 : 11;
+      wm = S.fw, um = S.fu, fb = lay_f(fl, t, 0);
+      if (exchange) {
+        __syncthreads();
+        const float2* bf = sm + pad(fb);
 #pragma unroll
-    for (int i = 0; i < 16; ++i) r[i] = bf[(i & 1) + (fl ? 68 : 544) * (i >> 1)];
+        for (int i = 0; i < 16; ++i) r[i] = bf[(i & 1) + (fl ? 68 : 544) * (i >> 1)];
+      }
+    }
+    reg_wht(r, ax, wm);
+    if (P.phase && S.phase_at == st) reg_phase(r, P, wt, s_tt, q0, lm, s_rt, fb);
+    reg_prod(r, P, s_rot, ax, um);
+    if (st == 0 && exchange) {
+      float2* b0p = sm + pad(2 * t);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) b0p[(i & 1) + 544 * (i >> 1)] = r[i];
+    } else if (st >= 1 && st <= S.nr) {
+      round_io_at<true>(sm, r, ax[0]);
+    }
   }
-  const int axf[4] = {0, fl ? 6 : 9, fl ? 7 : 10, fl ? 8 : 11};
-  reg_wht(r, axf, S.fw);
-  if (P.phase && S.phase_at == S.nr + 1) reg_phase(r, P, wt, s_tt, q0, lm, s_rt, lay_f(fl, t, 0));
-  reg_prod(r, P, s_rot, axf, S.fu);
   // Diagonal after the products (final layout L0 only), masses, store.
   if (P.dh) {
     const WindowSplit ws = window_split(wt, 256);
@@ -1302,7 +1303,7 @@ int launch_pass(const PassParams& Pin, cudaStream_t s) {
   // The register-first kernel: 12-bit tiles, the phase from pass tables, at most one
   // diagonal and not both the init and the phase.
   P.sched = TB == kTileBits && !(P.init && P.phase) && !(P.phase && !P.tt_phase) && !(P.dg && P.dh) &&
-            !g_fourier_legacy && plan_sched(P, P.s);
+            !(P.u_mask && !P.rot) && !g_fourier_legacy && plan_sched(P, P.s);
   P.top_axis = -1;
   for (int a = 0; a < TB; ++a)
     if ((a < P.c ? a : P.q + (a - P.c)) == P.m - 1) P.top_axis = a;
