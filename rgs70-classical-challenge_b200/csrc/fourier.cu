@@ -835,16 +835,6 @@ __global__ void __launch_bounds__(256, MINB)
         }
       }
     }
-  } else if (P.init) {
-    const u64 varying = ((1ull << P.c) - 1ull) | (((1ull << P.K) - 1ull) << P.q);
-    TileLut tl;
-    tile_lut(P.lut_z, P.chunks, base, varying, tl);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const u64 g = tile_global(P, tile, lay_f(0, t, 2 * k));
-      r[2 * k] = init_value(P, tl, g);
-      r[2 * k + 1] = init_value(P, tl, g + 1);
-    }
   } else if (TMA) {
     // The tile is in the staging buffer (dense, tile index order): wait for it, read it,
     // then refill the buffer with the next tile while this one is transformed.  A wait
@@ -1301,9 +1291,11 @@ int launch_pass(const PassParams& Pin, cudaStream_t s) {
   if (rc) return rc;
   PassParams P = Pin;
   // The register-first kernel: 12-bit tiles, the phase from pass tables, at most one
-  // diagonal and not both the init and the phase.
+  // diagonal, not both the init and the phase, the table init only, products as scaled
+  // rotations (the rest takes fourier_pass_kernel).
   P.sched = TB == kTileBits && !(P.init && P.phase) && !(P.phase && !P.tt_phase) && !(P.dg && P.dh) &&
-            !(P.u_mask && !P.rot) && !g_fourier_legacy && plan_sched(P, P.s);
+            !(P.u_mask && !P.rot) && !(P.init && !(P.init == INIT_COV_SPECIAL && P.tt_init)) && !g_fourier_legacy &&
+            plan_sched(P, P.s);
   P.top_axis = -1;
   for (int a = 0; a < TB; ++a)
     if ((a < P.c ? a : P.q + (a - P.c)) == P.m - 1) P.top_axis = a;
