@@ -735,6 +735,56 @@ __device__ __forceinline__ void tma_tile(const PassParams& P, const CUtensorMap&
 // which one thread prefetches the next tile with a tensor-map load into a dense staging
 // buffer while the block transforms the current one; the load stage then reads the tile
 // from shared memory (16-byte accesses, layout L0) instead of from HBM.
+// Per-tile constants of the register-first kernel, computed by one full warp in one round
+// trip to memory (the block waits for them at its first barrier): one lane per 8-bit
+// chunk of the tile base loads that chunk's table entry and the entries are combined by
+// shuffles.  tile_consts: b(base) and q(base) of a pass table (XOR over the chunks) and
+// the cross-term mask L of the tile axes; diag_base: the diagonal's factor D(base)
+// (product over the chunks, lane 0's value broadcast so every lane holds the same).
+__device__ __forceinline__ void tile_consts(const PassParams& P, const u64* lut, const u64* qsym, u64 base, bool map,
+                                            u64& b0, int& q0, unsigned& lm) {
+  const int lane = threadIdx.x & 31;
+  u64 b = 0, pm = 0;
+  if (lane < P.chunks) {
+    const u64* e = lut + ((((u64)lane << 8) + ((base >> (8 * lane)) & 255ull)) << 1);
+    if (map) b = __ldg(e);
+    pm = __ldg(e + 1);
+  }
+#pragma unroll
+  for (int off = 4; off; off >>= 1) {
+    b ^= __shfl_xor_sync(0xffffffffu, b, off);
+    pm ^= __shfl_xor_sync(0xffffffffu, pm, off);
+  }
+  const unsigned bitv = lane < kTileBits ? (__popcll(__ldg(qsym + local_to_global_bit(P, lane)) & base) & 1) : 0u;
+  lm = __ballot_sync(0xffffffffu, bitv);
+  b0 = b;
+  q0 = __popcll(pm & (base | (1ull << 63))) & 1;
+}
+
+__device__ __forceinline__ float2 diag_base(const PassParams& P, const float2* T, u64 base) {
+  const int lane = threadIdx.x & 31;
+  float2 d = make_float2(1.f, 0.f);
+  if (lane < P.chunks) d = __ldg(T + ((u64)lane << 8) + ((base >> (8 * lane)) & 255ull));
+#pragma unroll
+  for (int off = 4; off; off >>= 1)
+    d = cmulf(d, make_float2(__shfl_xor_sync(0xffffffffu, d.x, off), __shfl_xor_sync(0xffffffffu, d.y, off)));
+  return make_float2(__shfl_sync(0xffffffffu, d.x, 0), __shfl_sync(0xffffffffu, d.y, 0));
+}
+
+// Window tables (see window_tables) by two full warps: entry e = thread - 32 < 48.
+__device__ __forceinline__ void window_tables_warps(float2 (*wt)[16], const PassParams& P, const float2* T,
+                                                    const float2* ratio, u64 base) {
+  const float2 d = diag_base(P, T, base);
+  const int e = (int)threadIdx.x - 32;
+  if (e >= 48) return;
+  const int w = e >> 4, i = e & 15;
+  float2 v = w == 0 ? d : make_float2(1.f, 0.f);
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+    if ((i >> a) & 1) v = cmulf(v, __ldg(ratio + local_to_global_bit(P, 4 * w + a)));
+  wt[w][i] = v;
+}
+
 template <int MINB, bool W64, bool TMA>
 __global__ void __launch_bounds__(256, MINB)
     fourier_sched_kernel(const __grid_constant__ PassParams P, const __grid_constant__ CUtensorMap tmap) {
@@ -768,15 +818,37 @@ __global__ void __launch_bounds__(256, MINB)
   const u64 tile = it + P.tile0;
   const u64 base = tile_global(P, tile, 0);
   if (TMA) __syncthreads();  // the previous tile's readers of the shared tables and buffers are done
-  if (init_tab)
-    tile_tables_setup(P, P.tt_init, P.lut_z, P.qsym_z, base, kTileBits, true, s_tt, s_b0, s_q0, s_lm);
-  else if (P.phase)
-    tile_tables_setup(P, P.tt_phase, P.lut_a, P.qsym_a, base, kTileBits, false, s_tt, s_b0, s_q0, s_lm);
-  if (P.dg)
-    window_tables(wt, P, P.dg, P.rg, base, kTileBits);
-  else if (P.dh)
-    window_tables(wt, P, P.dh, P.rh, base, kTileBits);
-  if (P.rot && t >= 64 && t < 64 + kTileBits) s_rot[t - 64] = __ldg(P.rot + local_to_global_bit(P, t - 64));
+  if (init_tab || P.phase) {
+    const TileTables* tt = init_tab ? P.tt_init : P.tt_phase;
+    for (int i = t; i < 128; i += 256) {
+      s_tt.qtab[i] = __ldg(&tt->qtab[i]);
+      if (init_tab && i < 64) {
+        s_tt.mlo[i] = __ldg(&tt->mlo[i]);
+        s_tt.mhi[i] = __ldg(&tt->mhi[i]);
+      }
+    }
+    if (t < 32) {
+      u64 b0;
+      int q0;
+      unsigned lm;
+      if (init_tab)
+        tile_consts(P, P.lut_z, P.qsym_z, base, true, b0, q0, lm);
+      else
+        tile_consts(P, P.lut_a, P.qsym_a, base, false, b0, q0, lm);
+      if (t == 0) {
+        s_b0 = b0;
+        s_q0 = q0;
+        s_lm = lm;
+      }
+    }
+  }
+  if (t >= 32 && t < 96) {
+    if (P.dg)
+      window_tables_warps(wt, P, P.dg, P.rg, base);
+    else if (P.dh)
+      window_tables_warps(wt, P, P.dh, P.rh, base);
+  }
+  if (P.rot && t >= 96 && t < 96 + kTileBits) s_rot[t - 96] = __ldg(P.rot + local_to_global_bit(P, t - 96));
   __syncthreads();
   const int q0 = s_q0;
   const unsigned lm = s_lm;
