@@ -86,6 +86,7 @@ struct PassSched {
   int fin_l1;                     // final layout L1 (else L0)
   unsigned fw, fu;
   int phase_at;                   // stage of the phase: 0 load, 1..nr rounds, nr + 1 final, -1 none
+  int ld_w0;                      // load stage: -1 layout L0, else the window [ld_w0, ld_w0 + 4) (computed init)
 };
 
 struct PassParams {
@@ -602,9 +603,9 @@ __device__ __forceinline__ void reg_prod(float2 (&r)[16], const PassParams& P, c
 
 // Register axes of the schedule's phase stage.
 __device__ __forceinline__ void phase_axes(const PassSched& S, int (&ax)[4]) {
-  const bool round = S.phase_at >= 1 && S.phase_at <= S.nr;
+  const bool round = (S.phase_at >= 1 && S.phase_at <= S.nr) || (S.phase_at == 0 && S.ld_w0 >= 0);
   const bool l1 = S.phase_at == S.nr + 1 && S.fin_l1;
-  const int w0 = round ? S.rw0[S.phase_at - 1] : 0;
+  const int w0 = S.phase_at == 0 ? S.ld_w0 : (round ? S.rw0[S.phase_at - 1] : 0);
 #pragma unroll
   for (int a = 0; a < 4; ++a) ax[a] = round ? w0 + a : (a == 0 ? 0 : (l1 ? 5 : 8) + a);
 }
@@ -785,7 +786,9 @@ __device__ __forceinline__ void window_tables_warps(float2 (*wt)[16], const Pass
   wt[w][i] = v;
 }
 
-template <int MINB, bool W64, bool TMA>
+// INIT = true: the init pass (table init computed in registers, nothing loaded), a
+// separate instantiation so the loading passes carry none of its code or registers.
+template <int MINB, bool W64, bool TMA, bool INIT>
 __global__ void __launch_bounds__(256, MINB)
     fourier_sched_kernel(const __grid_constant__ PassParams P, const __grid_constant__ CUtensorMap tmap) {
   using O = typename std::conditional<W64, u64, unsigned>::type;
@@ -804,7 +807,7 @@ __global__ void __launch_bounds__(256, MINB)
   const PassSched& S = P.s;
   const int t = threadIdx.x;
   const u64 ntl = P.ntiles ? P.ntiles : (1ull << (P.m - kTileBits));
-  const bool init_tab = P.init == INIT_COV_SPECIAL && P.tt_init;
+  constexpr bool init_tab = INIT;
   uint32_t phase = 0;
   if (TMA) {
     if (t == 0) {
@@ -857,7 +860,12 @@ __global__ void __launch_bounds__(256, MINB)
     // mask, the q_A phase's folded into its factors rt.
     if (t < 32) {
       int pax[4] = {0, 9, 10, 11};
-      if (!init_tab) phase_axes(S, pax);
+      if (!init_tab) {
+        phase_axes(S, pax);
+      } else if (S.ld_w0 >= 0) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a) pax[a] = S.ld_w0 + a;
+      }
       const int i = t & 15;
       int X = 0;
       float2 v = make_float2(1.f, 0.f);
@@ -875,8 +883,22 @@ __global__ void __launch_bounds__(256, MINB)
     __syncthreads();
   }
   float2 r[16];
-  // Load stage (L0): init computed in registers, or the state loaded.
-  if (init_tab) {
+  // Load stage: init computed in registers (layout L0 or a window), or the state loaded (L0).
+  if (init_tab && S.ld_w0 >= 0) {
+    const int w0 = S.ld_w0;
+    const int fb = round_f0(t, w0);
+    const int axw[4] = {w0, w0 + 1, w0 + 2, w0 + 3};
+    const unsigned sg = sign_mask(s_tt, q0, lm, fb, axw, s_qw);
+    const u64 b0 = s_b0;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const int f = fb | (i << w0);
+      const u64 b = b0 ^ s_tt.mlo[f & 63] ^ s_tt.mhi[(f >> 6) & 63];
+      const float2 w = W64 ? __ldg(P.wspecf + __popcll(b) * (P.m + 1) + __popcll(b & P.outmask))
+                           : __ldg(P.wspecf + __popc((unsigned)b) * (P.m + 1) + __popc((unsigned)(b & P.outmask)));
+      r[i] = ((sg >> i) & 1u) ? make_float2(-w.x, -w.y) : w;
+    }
+  } else if (init_tab) {
     const int ax0[4] = {0, 9, 10, 11};
     const unsigned sg = sign_mask(s_tt, q0, lm, 2 * t, ax0, s_qw);
     const u64 b0 = s_b0;
@@ -942,13 +964,17 @@ __global__ void __launch_bounds__(256, MINB)
   // one copy of the register operations (a rolled loop): the kernel's code stays small
   // enough for the instruction cache.
   const int fl = S.fin_l1;
-  const bool exchange = S.nr > 0 || fl;
+  const bool exchange = S.nr > 0 || fl || S.ld_w0 >= 0;
 #pragma unroll 1
   for (int st = 0; st <= S.nr + 1; ++st) {
     int ax[4];
     unsigned wm, um;
     int fb;
-    if (st == 0) {
+    if (st == 0 && S.ld_w0 >= 0) {
+      const int w0 = S.ld_w0;
+      ax[0] = w0, ax[1] = w0 + 1, ax[2] = w0 + 2, ax[3] = w0 + 3;
+      wm = S.ld_w, um = S.ld_u, fb = round_f0(t, w0);
+    } else if (st == 0) {
       ax[0] = 0, ax[1] = 9, ax[2] = 10, ax[3] = 11;
       wm = S.ld_w, um = S.ld_u, fb = 2 * t;
     } else if (st <= S.nr) {
@@ -970,7 +996,9 @@ __global__ void __launch_bounds__(256, MINB)
     reg_wht(r, ax, wm);
     if (P.phase && S.phase_at == st) reg_phase(r, P, wt, s_tt, q0, lm, s_rt, fb);
     reg_prod(r, P, s_rot, ax, um);
-    if (st == 0 && exchange) {
+    if (st == 0 && S.ld_w0 >= 0) {
+      round_io_at<true>(sm, r, S.ld_w0);
+    } else if (st == 0 && exchange) {
       float2* b0p = sm + pad(2 * t);
 #pragma unroll
       for (int i = 0; i < 16; ++i) b0p[(i & 1) + 544 * (i >> 1)] = r[i];
@@ -1281,14 +1309,18 @@ int set_smem_attr() {
   if (device >= 0 && device < 64 && done[device]) return RGS_OK;
   const int bytes = ((1 << kTileBits) + (1 << (kTileBits - 4))) * (int)sizeof(float2);
   RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_pass_kernel<MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_sched_kernel<MINB, false, false>,
+  RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_sched_kernel<MINB, false, false, false>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_sched_kernel<MINB, true, false>,
+  RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_sched_kernel<MINB, true, false, false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_sched_kernel<MINB, false, false, true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_sched_kernel<MINB, true, false, true>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   if (MINB == 3) {
-    RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_sched_kernel<3, false, true>,
+    RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_sched_kernel<3, false, true, false>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmemBytes));
-    RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_sched_kernel<3, true, true>,
+    RGS_CUDA_TRY(cudaFuncSetAttribute(fourier_sched_kernel<3, true, true, false>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmemBytes));
   }
   if (device >= 0 && device < 64) done[device] = true;
@@ -1298,19 +1330,21 @@ int set_smem_attr() {
 // One stage sequence of the register-first kernel for a given round count and final
 // layout: every axis goes to the earliest stage that holds it, the phase (or the
 // WHT -> products boundary) to the stage where the last WHT axis is done.
-bool simulate_sched(unsigned W, unsigned U, bool phase, int n, const int* w0, int fl, PassSched& T) {
+bool simulate_sched(unsigned W, unsigned U, bool phase, int n, const int* w0, int fl, int ldw, PassSched& T) {
   const unsigned R0 = 1u | (7u << 9), R1 = 1u | (7u << 6);
+  const unsigned Rl = ldw < 0 ? R0 : (15u << ldw);  // registers of the load stage
   T = PassSched{};
+  T.ld_w0 = ldw;
   bool pending = W != 0 || phase;
   unsigned Wr = W, Ur = U;
   T.phase_at = -1;
-  T.ld_w = Wr & R0;
-  Wr &= ~R0;
+  T.ld_w = Wr & Rl;
+  Wr &= ~Rl;
   if (pending && !Wr) {
     T.phase_at = 0;
     pending = false;
   }
-  T.ld_u = pending ? 0u : (Ur & R0);
+  T.ld_u = pending ? 0u : (Ur & Rl);
   Ur &= ~T.ld_u;
   T.nr = n;
   for (int j = 0; j < n; ++j) {
@@ -1336,20 +1370,28 @@ bool simulate_sched(unsigned W, unsigned U, bool phase, int n, const int* w0, in
 }
 
 // Fewest shared-memory rounds (windows w0 in 0..8, all conflict-free in the padded
-// layout), final layout L0 preferred; false when three rounds do not suffice.
+// layout), final layout L0 preferred; false when three rounds do not suffice.  A pass
+// that computes its tile (the init) may also hold any window in registers at the load
+// stage (its elements need no coalesced load), which saves the init pass a round.
 bool plan_sched(const PassParams& P, PassSched& S) {
   const bool phase = P.phase != 0;
+#ifdef RGS_NO_INIT_WINDOW
+  const int ldmax = -1;
+#else
+  const int ldmax = P.init ? 8 : -1;
+#endif
   for (int n = 0; n <= 3; ++n) {
     int count = 1;
     for (int j = 0; j < n; ++j) count *= 9;
-    for (int fl = 0; fl < 2; ++fl) {
-      if (fl && P.dh) continue;  // the diagonal after the products uses layout L0
-      for (int code = 0; code < count; ++code) {
-        int w0[3] = {0, 0, 0};
-        for (int j = 0, c = code; j < n; ++j, c /= 9) w0[j] = c % 9;
-        if (simulate_sched(P.wht_mask, P.u_mask, phase, n, w0, fl, S)) return true;
+    for (int ldw = -1; ldw <= ldmax; ++ldw)
+      for (int fl = 0; fl < 2; ++fl) {
+        if (fl && P.dh) continue;  // the diagonal after the products uses layout L0
+        for (int code = 0; code < count; ++code) {
+          int w0[3] = {0, 0, 0};
+          for (int j = 0, c = code; j < n; ++j, c /= 9) w0[j] = c % 9;
+          if (simulate_sched(P.wht_mask, P.u_mask, phase, n, w0, fl, ldw, S)) return true;
+        }
       }
-    }
   }
   return false;
 }
@@ -1386,17 +1428,28 @@ int launch_pass(const PassParams& Pin, cudaStream_t s) {
       RGS_CUDA_TRY(cudaGetDevice(&dev));
       const unsigned grid = (unsigned)std::min<u64>(tiles, (u64)3 * sm_count(dev));
       if (w64)
-        fourier_sched_kernel<3, true, true><<<grid, 256, kTmaSmemBytes, s>>>(P, map);
+        fourier_sched_kernel<3, true, true, false><<<grid, 256, kTmaSmemBytes, s>>>(P, map);
       else
-        fourier_sched_kernel<3, false, true><<<grid, 256, kTmaSmemBytes, s>>>(P, map);
+        fourier_sched_kernel<3, false, true, false><<<grid, 256, kTmaSmemBytes, s>>>(P, map);
+    } else if (P.init) {
+      // The table init (the only init this kernel takes, see P.sched above).
+      const unsigned g = (unsigned)tiles;
+      if (P.variant && w64)
+        fourier_sched_kernel<4, true, false, true><<<g, 256, smem, s>>>(P, map);
+      else if (P.variant)
+        fourier_sched_kernel<4, false, false, true><<<g, 256, smem, s>>>(P, map);
+      else if (w64)
+        fourier_sched_kernel<3, true, false, true><<<g, 256, smem, s>>>(P, map);
+      else
+        fourier_sched_kernel<3, false, false, true><<<g, 256, smem, s>>>(P, map);
     } else if (P.variant && w64) {
-      fourier_sched_kernel<4, true, false><<<(unsigned)tiles, 256, smem, s>>>(P, map);
+      fourier_sched_kernel<4, true, false, false><<<(unsigned)tiles, 256, smem, s>>>(P, map);
     } else if (P.variant) {
-      fourier_sched_kernel<4, false, false><<<(unsigned)tiles, 256, smem, s>>>(P, map);
+      fourier_sched_kernel<4, false, false, false><<<(unsigned)tiles, 256, smem, s>>>(P, map);
     } else if (w64) {
-      fourier_sched_kernel<3, true, false><<<(unsigned)tiles, 256, smem, s>>>(P, map);
+      fourier_sched_kernel<3, true, false, false><<<(unsigned)tiles, 256, smem, s>>>(P, map);
     } else {
-      fourier_sched_kernel<3, false, false><<<(unsigned)tiles, 256, smem, s>>>(P, map);
+      fourier_sched_kernel<3, false, false, false><<<(unsigned)tiles, 256, smem, s>>>(P, map);
     }
   } else if (P.variant) {
     fourier_pass_kernel<4><<<(unsigned)tiles, 1 << (TB - 4), smem, s>>>(P);
