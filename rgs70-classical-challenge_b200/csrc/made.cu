@@ -29,10 +29,12 @@ int fourier_tma_timeout(int* timed_out);
 namespace {
 
 // CTA tile of the tensor-core GEMM: 128 x 128 outputs (one TMEM accumulator of 128 lanes
-// x 128 fp32 columns), K in slices of 64, two shared-memory stages.
-constexpr int TBM = 128, TBN = 128, TBK = 64, kStages = 2;
+// x 128 fp32 columns), K in slices of 64.  Operands staged by the threads use two
+// shared-memory stages; TMA-loaded operands a three-stage pipeline (the loads of slices
+// k + 1 and k + 2 in flight while slice k is multiplied), two CTAs per SM.
+constexpr int TBM = 128, TBN = 128, TBK = 64, kStages = 2, kTmaStages = 3;
 constexpr int kTileBytes = TBM * TBK * 2;  // one 128 x 64 bf16 operand tile (16 KiB)
-constexpr int kGemmSmem = kStages * 2 * kTileBytes + 1024 + 64;
+constexpr int kGemmSmem = kTmaStages * 2 * kTileBytes + 1024 + 64;
 
 // Byte offset of the 16-byte chunk (row r, k-chunk kc) of a 128 x 64 operand tile in the
 // K-major no-swizzle layout: core matrices of 8 rows x 16 bytes, the eight k-chunks of a
@@ -124,15 +126,15 @@ struct GemmMaps {
 __global__ void __launch_bounds__(128) gemm_tc_kernel(GemmArgs g, const __grid_constant__ GemmMaps maps) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kStages * 2 * kTileBytes);  // done[2], full[2]
-  uint64_t* full = bars + kStages;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kTmaStages * 2 * kTileBytes);  // done[3], full[3]
+  uint64_t* full = bars + kTmaStages;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kTmaStages);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.y * TBM, n0 = blockIdx.x * TBN;
   const bool tma = maps.tma_a || maps.tma_b;
   const uint32_t tx_bytes = (maps.tma_a ? kTileBytes : 0) + (maps.tma_b ? kTileBytes : 0);
   if (threadIdx.x == 0) {
-    for (int s = 0; s < 2 * kStages; ++s) tc::mbar_init(&bars[s], 1);
+    for (int s = 0; s < 2 * kTmaStages; ++s) tc::mbar_init(&bars[s], 1);
     tc::fence_barrier_init();
   }
   if (warp == 0) tc::tmem_alloc(tmem_slot, TBN);
@@ -145,6 +147,52 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(GemmArgs g, const __grid_c
   const int KT = (g.K + TBK - 1) / TBK;
   const uint32_t idesc = tc::instr_desc(TBM, TBN, 1);
   bool ok = true;
+  if (maps.tma_a && maps.tma_b) {
+    // One thread issues the loads kTmaStages slices ahead and the MMAs; a stage is refilled
+    // once the MMAs that read it have completed (its done barrier).  Every wait is bounded;
+    // after one gives up, the loads still in flight and the last MMAs are waited for (also
+    // bounded) before the block frees its TMEM.
+    if (threadIdx.x == 0) {
+      int issued = 0, consumed = 0, committed = -1;
+      auto issue = [&](int kt) {
+        const int s = kt % kTmaStages;
+        unsigned char* As = base + s * 2 * kTileBytes;
+        tc::mbar_expect_tx(&full[s], 2 * kTileBytes);
+        tc::tma_load_2d(As, &maps.a, kt * TBK, m0, &full[s]);
+        tc::tma_load_2d(As + kTileBytes, &maps.b, kt * TBK, n0, &full[s]);
+        ++issued;
+      };
+      for (int kt = 0; kt < KT && kt < kTmaStages; ++kt) issue(kt);
+      for (int kt = 0; kt < KT; ++kt) {
+        const int s = kt % kTmaStages;
+        const uint32_t ph = (uint32_t)(kt / kTmaStages) & 1u;
+        if (!tc::mbar_wait(&full[s], ph)) {
+          ok = false;
+          break;
+        }
+        ++consumed;
+        tc::fence_after_sync();
+        const uint32_t a0 = tc::smem_u32(base + s * 2 * kTileBytes), b0 = a0 + kTileBytes;
+#pragma unroll
+        for (int k = 0; k < TBK / 16; ++k)
+          tc::mma_f16(tmem, tc::smem_desc(a0 + k * 32, 16, 1024, 2), tc::smem_desc(b0 + k * 32, 16, 1024, 2), idesc,
+                      (kt > 0 || k > 0) ? 1u : 0u);
+        tc::mma_commit(&bars[s]);
+        committed = kt;
+        if (kt + kTmaStages < KT) {
+          if (!tc::mbar_wait(&bars[s], ph)) {
+            ok = false;
+            break;
+          }
+          issue(kt + kTmaStages);
+        }
+      }
+      if (committed >= 0 && !tc::mbar_wait(&bars[committed % kTmaStages], (uint32_t)(committed / kTmaStages) & 1u))
+        ok = false;
+      if (!ok)
+        for (int kt = consumed; kt < issued; ++kt) tc::mbar_wait(&full[kt % kTmaStages], (uint32_t)(kt / kTmaStages) & 1u);
+    }
+  } else {
   for (int kt = 0; kt < KT; ++kt) {
     const int s = kt & 1;
     if (kt >= kStages && !tc::mbar_wait(&bars[s], (uint32_t)((kt >> 1) - 1) & 1u)) ok = false;
@@ -184,6 +232,7 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(GemmArgs g, const __grid_c
     }
   }
   if (ok && KT > 0 && !tc::mbar_wait(&bars[(KT - 1) & 1], (uint32_t)((KT - 1) >> 1) & 1u)) ok = false;
+  }
   ok = __syncthreads_and(ok);
   tc::fence_after_sync();
   if (ok) {
@@ -193,6 +242,21 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(GemmArgs g, const __grid_c
       tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
       tc::tmem_ld_wait();
       if (m >= g.M) continue;
+      if (g.C && !g.Cb && !g.mask && !g.gate && n0 + c0 + 16 <= g.N && (g.ldc & 3) == 0 &&
+          (((uintptr_t)g.C) & 15) == 0) {
+        // 16 consecutive columns of row m: four 16-byte stores.
+        float v[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          v[j] = __uint_as_float(r[j]) * g.alpha;
+          if (g.bias) v[j] += g.bias[n0 + c0 + j];
+          if (g.relu) v[j] = fmaxf(v[j], 0.f);
+        }
+        float4* dst = reinterpret_cast<float4*>(g.C + (size_t)m * g.ldc + n0 + c0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        continue;
+      }
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
         const int n = n0 + c0 + j;
