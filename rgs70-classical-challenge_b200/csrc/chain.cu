@@ -215,7 +215,24 @@ __global__ void chain_decide_kernel(const double* __restrict__ partial, int nblo
   double g0 = 1.0, g1 = 1.0, g2 = 0.0, g3 = 0.0;
   if (!analytic) {
     g0 = g1 = 0.0;
-    for (int k = threadIdx.x; k < nblocks; k += blockDim.x) {
+    // The first kLoadsAhead partials of this thread are loaded before any is summed (one
+    // memory round trip instead of one per partial); the sums keep the order k = t, t + 128, ...
+    constexpr int kLoadsAhead = 4;
+    double4 pk[kLoadsAhead];
+#pragma unroll
+    for (int q = 0; q < kLoadsAhead; ++q) {
+      const int k = threadIdx.x + q * (int)blockDim.x;
+      if (k < nblocks) pk[q] = *reinterpret_cast<const double4*>(partial + ((size_t)k * Bt + b) * 4);
+    }
+#pragma unroll
+    for (int q = 0; q < kLoadsAhead; ++q) {
+      if (threadIdx.x + q * (int)blockDim.x >= nblocks) break;
+      g0 += pk[q].x;
+      g1 += pk[q].y;
+      g2 += pk[q].z;
+      g3 += pk[q].w;
+    }
+    for (int k = threadIdx.x + kLoadsAhead * (int)blockDim.x; k < nblocks; k += blockDim.x) {
       const double4 p = *reinterpret_cast<const double4*>(partial + ((size_t)k * Bt + b) * 4);
       g0 += p.x;
       g1 += p.y;
