@@ -79,3 +79,33 @@ def test_device_modes_cover_every_step(pkg):
         for st in plan.steps:
             assert len(st.kernel) <= 2
             assert st.r_out >= st.r_in - 1 and st.r_out <= st.r_in + 1
+
+
+def test_chain_launch_count_host_logic(pkg):
+    """rgs_chain_launch_count (the chain sampler's kernel launches, counted on the host):
+    whole batch tiles, one bit-clearing kernel in sampling but not in marginals mode, one
+    log p zeroing kernel when log p is asked for, and per position at most a Gram pass, a
+    decision and a step (a fused pair shares the step)."""
+    import ctypes
+    rng = np.random.default_rng(11)
+    L = pkg._lib.lib()
+
+    def count(plan, n_items, tile, marginals, logp):
+        out = ctypes.c_int64()
+        pkg._lib.check(L.rgs_chain_launch_count(plan.handle, n_items, tile, marginals, logp, ctypes.byref(out)))
+        return out.value
+
+    for _ in range(10):
+        n = int(rng.integers(4, 30))
+        g = np.triu((rng.random((n, n)) < 0.25).astype(np.uint8), 1)
+        edges = list(zip(*map(list, np.nonzero(g))))
+        plan = pkg.ScanPlan(n, edges, rng.permutation(n).tolist())
+        one = count(plan, 32, 32, 0, 1)
+        assert count(plan, 0, 32, 0, 1) == 0
+        assert count(plan, 3 * 32, 32, 0, 1) == 3 * one
+        assert count(plan, 3 * 32 + 1, 32, 0, 1) == 4 * one
+        assert count(plan, 32, 32, 1, 1) == one - 1
+        assert count(plan, 32, 32, 0, 0) == one - 1
+        assert 2 * n - len(plan.pairs) + 1 <= one - 2 <= 3 * n + 1
+    with pytest.raises(ValueError):
+        count(pkg.ScanPlan(4, [(0, 1)], [0, 1, 2, 3]), -1, 32, 0, 1)
