@@ -16,10 +16,11 @@
 // elements in registers along 4 tile axes and applies every 2x2 operation on those axes.
 // fourier_sched_kernel (12-bit tiles) transforms the axes that sit in registers right
 // after the load and before the store there, and the rest in at most three padded
-// shared-memory rounds chosen per pass by the host (plan_sched); its loading passes stage
-// each next tile with a tensor-map (TMA) load while the current one is transformed.
-// fourier_pass_kernel (tiles of fewer bits, the generic phase path) runs one round per
-// four axes.  The whole transform is
+// shared-memory rounds chosen per pass by the host (plan_sched); optionally
+// (rgs_fourier_set_tma) its loading passes stage each next tile with a tensor-map (TMA)
+// load while the current one is transformed.  fourier_pass_kernel (tiles of fewer bits,
+// the generic chunk init, general 2x2 products) runs one round per four axes.  The whole
+// transform is
 //   pass 0          : init (computed, not loaded) + WHT on bits [0, 12)
 //   strided passes  : WHT on the next groups of <= 9 bits (balanced)
 //   middle pass     : WHT on the last group, q_A phase, products on that group
